@@ -26,6 +26,10 @@
 extern "C" {
 #endif
 
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
 /* ---------------------------------------------------------------- status */
 enum ss_status {
   SS_OK = 0,
@@ -259,6 +263,15 @@ int ss_realization_setup(const ss_run_config* config, uint64_t index,
                          int32_t* nspins, double* fields, int32_t* pairs,
                          double* couplings, int32_t* npairs, double* psi0);
 
+/* ------------------------------------------------------ plain FP64 path
+ * runRealization (io/Experiment.cpp:10-55) + Sequence::run
+ * (src/sequence/Sequence.cpp:69-106) for one realisation: the program is
+ * interpreted on the host and every step runs on the device in FP64, with
+ * one Propagator::evolve per Evolve step for the state and the reference.
+ * times: points; values: points x width (see ss_batch_shape). */
+int ss_run_realization(ss_engine* engine, const ss_run_config* config,
+                       uint64_t index, double* times, double* values);
+
 /* -------------------------------------------------------- batched engine
  * Runs `count` realisations (indices first..first+count-1) of a whole
  * pulse program on the device, state and reference together, and returns
@@ -282,6 +295,12 @@ int ss_batch_download(ss_batch* batch, double* rows, double* times);
    all realisations), amplitudes processed per run, kernel launches. */
 int ss_batch_stats(const ss_batch* batch, int64_t* orders,
                    double* amplitude_orders, int64_t* launches);
+/* Bytes ss_batch_run moves host->device (inputs) and device->host (rows). */
+int ss_batch_io_bytes(const ss_batch* batch, int64_t* h2d, int64_t* d2h);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
 
 #ifdef __cplusplus
 }

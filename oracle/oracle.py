@@ -317,6 +317,12 @@ class Ref(_Lib):
                                             _d(times), _d(values), C.byref(secs)))
         return times[:p], values[: count * p * w].reshape(count, p, w), secs.value
 
+    def random_state(self, L: int, seed: int):
+        """The reference tests' randomState (DenseReference.cpp:204-214)."""
+        out = np.zeros(2 << L)
+        self._check(self.lib.refd_random_state(L, C.c_uint64(seed), _d(out)))
+        return out
+
     def run_experiment(self, cfg: SsRunConfig, threads: int):
         p, w = self.shape(cfg)
         times = np.zeros(max(p, 1))

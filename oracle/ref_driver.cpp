@@ -17,6 +17,7 @@
 #include <atomic>
 #include <chrono>
 #include <mutex>
+#include <random>
 
 #include "spinsim/core/Bessel.hpp"
 #include "spinsim/core/Chebyshev.hpp"
@@ -467,6 +468,23 @@ int refd_run_experiment(const ss_run_config* c, int threads, double* times, doub
     std::memcpy(mean, m.data(), sizeof(double) * m.size());
     std::memcpy(sd, s.data(), sizeof(double) * s.size());
     std::memcpy(se, e.data(), sizeof(double) * e.size());
+  });
+}
+
+// The test-state recipe of the reference's tests/DenseReference.cpp:204-214
+// (mt19937_64 seeded directly, standard normal re then im, normalised), so
+// the reference's own propagator cases can be replayed on the same states.
+int refd_random_state(int nspins, uint64_t seed, double* out) {
+  return guarded([&] {
+    StateVector psi(static_cast<std::size_t>(nspins));
+    std::mt19937_64 rng(seed);
+    std::normal_distribution<double> gauss(0.0, 1.0);
+    for (std::size_t k = 0; k < psi.size(); ++k) {
+      psi.re(k) = gauss(rng);
+      psi.im(k) = gauss(rng);
+    }
+    psi.normalize();
+    storeState(psi, out);
   });
 }
 

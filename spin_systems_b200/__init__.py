@@ -1,0 +1,470 @@
+"""spin_systems_b200 -- Python access to the B200 Chebyshev echo engine.
+
+The engine itself is native: CUDA kernels for sm_100a and C++ host code in
+``lib/libspinsim_b200.so``, behind the C ABI of ``include/spinsim_b200.h``.
+This module binds that ABI with ctypes and mirrors the reference's objects
+(spinsim's StateVector, Hamiltonian, Propagator, SpinRotation, observables)
+so tests and benchmarks read like the reference's own.  There is no Python or
+CPU fallback: without the built library every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import weakref
+from pathlib import Path
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import abi
+from .abi import SsRunConfig, SsObservable
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "lib" / "libspinsim_b200.so"
+HEADER = PKG.parent / "include" / "spinsim_b200.h"
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int32)
+_lib: Optional[C.CDLL] = None
+
+
+class SpinsimError(RuntimeError):
+    """A failed C ABI call: `.code` is the ss_status, `.kind` its name."""
+
+    def __init__(self, code: int, msg: str):
+        self.code = code
+        self.kind = abi.STATUS_NAMES.get(code, "unknown")
+        super().__init__(f"{self.kind}: {msg}")
+
+
+class ConvergenceError(SpinsimError):
+    pass
+
+
+class DomainError(SpinsimError):
+    pass
+
+
+class OutOfRangeError(SpinsimError):
+    pass
+
+
+class InvalidArgumentError(SpinsimError):
+    pass
+
+
+class NoDeviceError(SpinsimError):
+    pass
+
+
+_ERRORS = {1: InvalidArgumentError, 2: OutOfRangeError, 3: DomainError, 4: ConvergenceError,
+           9: NoDeviceError}
+
+
+def load(path: Path = LIB_PATH) -> C.CDLL:
+    """Loads the engine library (built in-tree by __graft_entry__.build())."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not path.exists():
+        raise FileNotFoundError(
+            f"{path} is missing: build the CUDA extension first (python -c "
+            "'import __graft_entry__ as g; g.build()')")
+    lib = C.CDLL(str(path))
+    lib.ss_last_error.restype = C.c_char_p
+    lib.ss_engine_stream.restype = C.c_void_p
+    lib.ss_engine_stream.argtypes = [C.c_void_p]
+    lib.ss_engine_launch_count.restype = C.c_int64
+    lib.ss_engine_launch_count.argtypes = [C.c_void_p]
+    for name in ("ss_state_scale",):
+        getattr(lib, name).argtypes = [C.c_void_p, C.c_double]
+    lib.ss_state_add_scaled.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_void_p]
+    lib.ss_axpy_sigma.argtypes = [C.c_double, C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+    lib.ss_axpy_coupling.argtypes = [C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_int,
+                                     C.c_int, C.c_void_p]
+    lib.ss_ham_apply.argtypes = [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_int]
+    lib.ss_evolve.argtypes = [C.c_void_p, C.c_void_p, _dp, C.c_int64, C.c_double, C.c_int,
+                              C.c_int64, C.c_int]
+    lib.ss_propagate.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_int64, C.c_int,
+                                 C.c_double, C.POINTER(C.c_int64)]
+    lib.ss_bessel.argtypes = [C.c_int, C.c_double, C.c_int64, _dp, C.POINTER(C.c_int64)]
+    lib.ss_chebyshev_build.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_int64, _dp,
+                                       C.c_int64, C.POINTER(C.c_int64), _dp]
+    lib.ss_rotation_matrix.argtypes = [_dp, C.c_double, _dp]
+    lib.ss_state_set_basis.argtypes = [C.c_void_p, C.c_uint64]
+    lib.ss_realization_setup.argtypes = [C.POINTER(SsRunConfig), C.c_uint64, _ip, _dp, _ip, _dp,
+                                         _ip, _dp]
+    lib.ss_batch_create.argtypes = [C.c_void_p, C.POINTER(SsRunConfig), C.c_uint64, C.c_int64,
+                                    C.c_int, C.POINTER(C.c_void_p)]
+    lib.ss_run_realization.argtypes = [C.c_void_p, C.POINTER(SsRunConfig), C.c_uint64, _dp, _dp]
+    _lib = lib
+    return lib
+
+
+def check(rc: int) -> None:
+    if rc:
+        msg = load().ss_last_error().decode()
+        raise _ERRORS.get(rc, SpinsimError)(rc, msg)
+
+
+def _d(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+def _i(a: np.ndarray):
+    return a.ctypes.data_as(_ip)
+
+
+def header_symbols() -> list:
+    """Every function the public header declares."""
+    import re
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"^(?:int|const char\*|void\*|int64_t)\s+(ss_\w+)\(", text, re.M)))
+
+
+# ------------------------------------------------------------------ engine
+class Engine:
+    """One device and its stream (ss_engine_create)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load()
+        h = C.c_void_p()
+        check(self.lib.ss_engine_create(device, C.byref(h)))
+        self.handle = h
+        self._children = weakref.WeakSet()
+
+    def _adopt(self, child) -> None:
+        self._children.add(child)
+
+    def close(self) -> None:
+        """Destroys every object still alive on this engine, then the engine
+        (the C ABI requires states, Hamiltonians and batches to go first)."""
+        if self.handle:
+            for child in list(self._children):
+                child._destroy()
+            check(self.lib.ss_engine_destroy(self.handle))
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def synchronize(self) -> None:
+        check(self.lib.ss_engine_synchronize(self.handle))
+
+    @property
+    def stream(self) -> int:
+        return self.lib.ss_engine_stream(self.handle)
+
+    @property
+    def launches(self) -> int:
+        return self.lib.ss_engine_launch_count(self.handle)
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class StateVector:
+    """2^L complex amplitudes on the device (core/StateVector.hpp:82-140)."""
+
+    def __init__(self, engine: Engine, nspins: int, data: Optional[np.ndarray] = None):
+        self.engine, self.lib, self.nspins = engine, engine.lib, nspins
+        h = C.c_void_p()
+        check(self.lib.ss_state_create(engine.handle, nspins, C.byref(h)))
+        self.handle = h
+        engine._adopt(self)
+        if data is not None:
+            self.upload(data)
+
+    def _destroy(self) -> None:
+        if getattr(self, "handle", None):
+            self.lib.ss_state_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self._destroy()
+        except Exception:
+            pass
+
+    @property
+    def size(self) -> int:
+        return 1 << self.nspins
+
+    def upload(self, data: np.ndarray) -> None:
+        a = np.ascontiguousarray(data, dtype=np.float64)
+        assert a.size == 2 * self.size
+        check(self.lib.ss_state_upload(self.handle, _d(a)))
+
+    def download(self) -> np.ndarray:
+        out = np.empty(2 * self.size)
+        check(self.lib.ss_state_download(self.handle, _d(out)))
+        return out
+
+    def copy_from(self, other: "StateVector") -> None:
+        check(self.lib.ss_state_copy(self.handle, other.handle))
+
+    def set_zero(self) -> None:
+        check(self.lib.ss_state_set_zero(self.handle))
+
+    def scale(self, f: float) -> None:
+        check(self.lib.ss_state_scale(self.handle, f))
+
+    def negate(self) -> None:
+        check(self.lib.ss_state_negate(self.handle))
+
+    def add_scaled(self, cr: float, ci: float, other: "StateVector") -> None:
+        check(self.lib.ss_state_add_scaled(self.handle, cr, ci, other.handle))
+
+    def set_basis_state(self, index: int) -> None:
+        check(self.lib.ss_state_set_basis(self.handle, index))
+
+    def norm(self) -> float:
+        out = C.c_double()
+        check(self.lib.ss_state_norm(self.handle, C.byref(out)))
+        return out.value
+
+    def normalize(self) -> float:
+        out = C.c_double()
+        check(self.lib.ss_state_normalize(self.handle, C.byref(out)))
+        return out.value
+
+    def inner_product(self, other: "StateVector"):
+        out = (C.c_double * 2)()
+        check(self.lib.ss_state_inner_product(self.handle, other.handle, out))
+        return out[0], out[1]
+
+    def swap(self, other: "StateVector") -> None:
+        check(self.lib.ss_state_swap(self.handle, other.handle))
+
+
+# Pauli kernels (core/SpinOperators.hpp:22-58)
+def axpy_sigma(c: float, src: StateVector, spin: int, axis: int, dst: StateVector) -> None:
+    check(src.lib.ss_axpy_sigma(c, src.handle, spin, axis, dst.handle))
+
+
+def apply_sigma(src: StateVector, spin: int, axis: int, dst: StateVector) -> None:
+    check(src.lib.ss_apply_sigma(src.handle, spin, axis, dst.handle))
+
+
+def axpy_coupling(jx, jy, jz, src: StateVector, a: int, b: int, dst: StateVector) -> None:
+    check(src.lib.ss_axpy_coupling(jx, jy, jz, src.handle, a, b, dst.handle))
+
+
+def apply_total_spin(axis: int, src: StateVector, dst: StateVector) -> None:
+    check(src.lib.ss_apply_total_spin(axis, src.handle, dst.handle))
+
+
+class Hamiltonian:
+    """Fields and couplings on the device (core/Hamiltonian.hpp:32-110)."""
+
+    def __init__(self, engine: Engine, nspins: int, fields=None, pairs=None, couplings=None):
+        self.engine, self.lib, self.nspins = engine, engine.lib, nspins
+        h = C.c_void_p()
+        check(self.lib.ss_ham_create(engine.handle, nspins, C.byref(h)))
+        self.handle = h
+        engine._adopt(self)
+        self.set_terms(np.zeros(3 * nspins) if fields is None else fields,
+                       np.zeros(0, dtype=np.int32) if pairs is None else pairs,
+                       np.zeros(0) if couplings is None else couplings)
+
+    def _destroy(self) -> None:
+        if getattr(self, "handle", None):
+            self.lib.ss_ham_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self._destroy()
+        except Exception:
+            pass
+
+    def set_terms(self, fields, pairs, couplings) -> None:
+        f = np.ascontiguousarray(fields, dtype=np.float64)
+        p = np.ascontiguousarray(pairs, dtype=np.int32)
+        j = np.ascontiguousarray(couplings, dtype=np.float64)
+        check(self.lib.ss_ham_set_terms(self.handle, _d(f), len(p) // 2, _i(p), _d(j)))
+
+    def set_fields(self, fields) -> None:
+        f = np.ascontiguousarray(fields, dtype=np.float64)
+        check(self.lib.ss_ham_set_fields(self.handle, _d(f)))
+
+    def spectral_bound(self) -> float:
+        out = C.c_double()
+        check(self.lib.ss_ham_spectral_bound(self.handle, C.byref(out)))
+        return out.value
+
+    def apply(self, scale: float, src: StateVector, dst: StateVector, accumulate: bool) -> None:
+        check(self.lib.ss_ham_apply(self.handle, scale, src.handle, dst.handle, int(accumulate)))
+
+    def apply_physical(self, src: StateVector, dst: StateVector) -> None:
+        self.apply(1.0, src, dst, False)
+
+    def apply_twice_normalized(self, bound: float, src: StateVector, dst: StateVector) -> None:
+        if not bound > 0:
+            raise DomainError(3, "spectral bound must be positive")
+        self.apply(-2.0 / bound, src, dst, False)
+
+
+def bessel(kind: int, x: float, count: int):
+    lib = load()
+    out = np.zeros(count)
+    nz = C.c_int64()
+    check(lib.ss_bessel(kind, x, count, _d(out), C.byref(nz)))
+    return out, nz.value
+
+
+def chebyshev(mode: int, bound: float, tau: float, epsilon: float, max_order: int = 6000):
+    lib = load()
+    cap = max_order + 8
+    out = np.zeros(cap)
+    order = C.c_int64()
+    eb = C.c_double()
+    check(lib.ss_chebyshev_build(mode, bound, tau, epsilon, max_order, _d(out), cap,
+                                 C.byref(order), C.byref(eb)))
+    return out[: order.value + 1].copy(), eb.value
+
+
+class Propagator:
+    """Propagator::evolve (src/core/Propagator.cpp:75-100) on the device."""
+
+    def __init__(self, nspins: int, epsilon: float = 1e-7):
+        if not epsilon > 0:
+            raise InvalidArgumentError(1, "epsilon must be positive")
+        self.nspins, self.epsilon, self.last_order = nspins, epsilon, 0
+
+    def evolve(self, ham: Hamiltonian, mode: int, psi: StateVector, tau: float, nsteps: int,
+               autonormalize: bool = False) -> None:
+        if psi.nspins != ham.nspins:
+            raise InvalidArgumentError(1, "state and Hamiltonian disagree on spin count")
+        if psi.nspins != self.nspins:
+            raise InvalidArgumentError(1, "state does not match the propagator's size")
+        order = C.c_int64(0)
+        check(ham.lib.ss_propagate(ham.handle, psi.handle, mode, tau, nsteps, int(autonormalize),
+                                   self.epsilon, C.byref(order)))
+        if nsteps:
+            self.last_order = order.value
+
+
+def rotation_matrix(axis: Sequence[float], angle: float) -> np.ndarray:
+    u = np.zeros(8)
+    ax = np.asarray(axis, dtype=np.float64)
+    check(load().ss_rotation_matrix(_d(ax), angle, _d(u)))
+    return u
+
+
+def rotate(psi: StateVector, axis, angle: float, targets) -> None:
+    """SpinRotation::apply (src/core/Gate.cpp:60-85)."""
+    u = rotation_matrix(axis, angle)
+    t = np.ascontiguousarray(targets, dtype=np.int32)
+    check(psi.lib.ss_rotate(psi.handle, _d(u), _i(t), len(t)))
+
+
+def two_spin_gate(psi: StateVector, m, a: int, b: int) -> None:
+    mm = np.ascontiguousarray(m, dtype=np.float64)
+    check(psi.lib.ss_two_spin_gate(psi.handle, _d(mm), a, b))
+
+
+def measure_corr(psi: StateVector, ref: StateVector, axis: int):
+    out = (C.c_double * 2)()
+    check(psi.lib.ss_measure_corr(psi.handle, ref.handle, axis, out))
+    return out[0], out[1]
+
+
+def measure_mag(psi: StateVector, spin: int, axis: int) -> float:
+    out = C.c_double()
+    check(psi.lib.ss_measure_mag(psi.handle, spin, axis, C.byref(out)))
+    return out.value
+
+
+def measure_energy(ham: Hamiltonian, psi: StateVector) -> float:
+    out = C.c_double()
+    check(psi.lib.ss_measure_energy(ham.handle, psi.handle, C.byref(out)))
+    return out.value
+
+
+def realization_setup(cfg: SsRunConfig, index: int, lmax: int):
+    """ss_realization_setup: the realisation's fields, couplings and psi0."""
+    lib = load()
+    n = 1 << lmax
+    fields = np.zeros(3 * lmax)
+    pairs = np.zeros(lmax * (lmax - 1) + 2, dtype=np.int32)
+    J = np.zeros(3 * (lmax * (lmax - 1) // 2) + 3)
+    psi0 = np.zeros(2 * n)
+    L, P = C.c_int32(), C.c_int32()
+    check(lib.ss_realization_setup(C.byref(cfg), index, C.byref(L), _d(fields), _i(pairs), _d(J),
+                                   C.byref(P), _d(psi0)))
+    L, P = L.value, P.value
+    return dict(L=L, fields=fields[: 3 * L].copy(), pairs=pairs[: 2 * P].copy(),
+                J=J[: 3 * P].copy(), psi0=psi0[: 2 << L].copy())
+
+
+def run_realization(engine: Engine, cfg: SsRunConfig, index: int, points: int, width: int):
+    """The plain FP64 path for one realisation (ss_run_realization)."""
+    times = np.zeros(max(points, 1))
+    values = np.zeros(max(points * width, 1))
+    check(engine.lib.ss_run_realization(engine.handle, C.byref(cfg), index, _d(times), _d(values)))
+    return times[:points], values[: points * width].reshape(points, width)
+
+
+class Batch:
+    """The batched engine (ss_batch_*): many realisations of one program."""
+
+    def __init__(self, engine: Engine, cfg: SsRunConfig, first: int, count: int,
+                 precision: int = abi.MIXED):
+        self.engine, self.lib = engine, engine.lib
+        self._cfg = cfg
+        h = C.c_void_p()
+        check(self.lib.ss_batch_create(engine.handle, C.byref(cfg), first, count, precision,
+                                       C.byref(h)))
+        self.handle = h
+        engine._adopt(self)
+        p, w = C.c_int64(), C.c_int64()
+        check(self.lib.ss_batch_shape(self.handle, C.byref(p), C.byref(w)))
+        self.points, self.width, self.count = p.value, w.value, count
+
+    def _destroy(self) -> None:
+        if getattr(self, "handle", None):
+            self.lib.ss_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self._destroy()
+        except Exception:
+            pass
+
+    def run(self):
+        rows = np.zeros(max(self.count * self.points * self.width, 1))
+        times = np.zeros(max(self.points, 1))
+        check(self.lib.ss_batch_run(self.handle, _d(rows), _d(times)))
+        return times[: self.points], rows[: self.count * self.points * self.width].reshape(
+            self.count, self.points, self.width)
+
+    def upload(self) -> None:
+        check(self.lib.ss_batch_upload(self.handle))
+
+    def execute(self) -> None:
+        check(self.lib.ss_batch_execute(self.handle))
+
+    def download(self):
+        rows = np.zeros(max(self.count * self.points * self.width, 1))
+        times = np.zeros(max(self.points, 1))
+        check(self.lib.ss_batch_download(self.handle, _d(rows), _d(times)))
+        return times[: self.points], rows[: self.count * self.points * self.width].reshape(
+            self.count, self.points, self.width)
+
+    def stats(self):
+        orders, amp, launches = C.c_int64(), C.c_double(), C.c_int64()
+        check(self.lib.ss_batch_stats(self.handle, C.byref(orders), C.byref(amp),
+                                      C.byref(launches)))
+        h2d, d2h = C.c_int64(), C.c_int64()
+        check(self.lib.ss_batch_io_bytes(self.handle, C.byref(h2d), C.byref(d2h)))
+        return dict(orders=orders.value, amplitude_orders=amp.value, launches=launches.value,
+                    h2d_bytes=h2d.value, d2h_bytes=d2h.value)

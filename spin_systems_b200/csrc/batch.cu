@@ -1,0 +1,1114 @@
+// The batched engine: many disorder realisations of one pulse program in one
+// persistent fused launch per system size, captured with its set-up as a CUDA
+// graph.  Host side: the program is linearised, every realisation is
+// assembled bit for bit as the reference does (geometry, disorder, psi0), and
+// each distinct Evolve step gets a per-realisation table (spectral bound,
+// Chebyshev series weights, prescaled couplings).  Device side: see
+// batch_kernel.cuh.
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <numeric>
+#include <thread>
+#include <tuple>
+
+#include "batch_kernel.cuh"
+#include "hamiltonian.cuh"
+
+namespace ss {
+
+void rotation_matrix(const double axis[3], double angle, double u[8]);
+void validate_config(const ss_run_config& c);
+
+namespace batch {
+namespace {
+
+constexpr int kPrepThreads = 256;
+
+// ---------------------------------------------------------------- device
+__device__ __forceinline__ double2 sigma_at(const double2* in, uint32_t k, int s, int axis) {
+  const uint32_t m = 1u << s;
+  if (axis == SS_AXIS_Z) {
+    const double2 a = in[k];
+    return (k & m) ? a : make_double2(-a.x, -a.y);
+  }
+  const double2 p = in[k ^ m];
+  if (axis == SS_AXIS_X) return p;
+  return (k & m) ? make_double2(p.y, -p.x) : make_double2(-p.y, p.x);
+}
+
+// psi0 -> state slot, reference = sum_s sigma_b(s) psi0 summed in spin order
+// (bit-identical to src/ensemble/Ensemble.cpp:47-58).
+__global__ void k_batch_prepare(const RealDev* reals, const double2* psi0, const long long* psi0_off,
+                                double2* states, int ref_axis) {
+  const RealDev rd = reals[blockIdx.x];
+  const uint32_t n = 1u << rd.L;
+  const double2* src = psi0 + psi0_off[blockIdx.x];
+  double2* st = states + rd.state_off;
+  for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) {
+    st[k] = src[k];
+    double re = 0.0, im = 0.0;
+    for (int s = 0; s < rd.L; ++s) {
+      const double2 v = sigma_at(src, k, s, ref_axis);
+      re += v.x;
+      im += v.y;
+    }
+    st[n + k] = make_double2(re, im);
+  }
+}
+
+template <int L, int R, typename Real, int PSI>
+__device__ void evolve_op(const Args& args, const Smem<Real>& sm, const RealDev& rd, double2* st,
+                          const Op& op, const TypeDev& ty) {
+  using Gm = Geo<L, R>;
+  using C2 = typename Cplx<Real>::T;
+  constexpr int NT = Gm::NT, NA = Gm::NA, G = Gm::G, N = Gm::N;
+  constexpr int bl = Gm::base(G - 1);  // = L - R: thread t owns k = t | a << bl
+  constexpr bool kMixed = std::is_same<Real, float>::value;
+  const uint32_t t = threadIdx.x;
+  const int P = rd.npairs;
+  const double* cb = args.cpool + ty.c_off;
+  const int2* pl = args.pairs + rd.pair_off;
+
+  __syncthreads();  // earlier readers of the coefficient tables are done
+  for (int i = t; i < L * L; i += NT) {
+    sm.cff[i] = Real(0);
+    sm.cfb[i] = Real(0);
+  }
+  __syncthreads();
+  for (int p = t; p < P; p += NT) {
+    const int2 q = pl[p];
+    sm.cff[q.x * L + q.y] = Real(cb[p]);
+    sm.cfb[q.x * L + q.y] = Real(cb[P + p]);
+  }
+  for (int s = t; s < L; s += NT) {
+    sm.ccx[s] = Real(cb[3 * P + L + s]);
+    sm.ccy[s] = Real(cb[3 * P + 2 * L + s]);
+  }
+  if (t == 0) {
+    int nc = 0;
+    if (kMixed) {
+      const double* ct = cb + 3 * P + 3 * L;
+      for (int c = 0; c < kCorr; ++c) {
+        const int pi = static_cast<int>(ct[4 * c]);
+        if (pi < 0) continue;
+        const int2 q = pl[pi];
+        sm.corr_mask[nc] = make_uint2(1u << q.x, 1u << q.y);
+        sm.corr_coef[nc] = make_double2(ct[4 * c + 1], ct[4 * c + 2]);
+        ++nc;
+      }
+    }
+    *sm.corr_n = nc;
+  }
+  // Scaled diagonal of this thread's amplitudes in FP64, summed in the
+  // reference's order (src/core/Hamiltonian.cpp:54-80).
+  double dg[NA];
+#pragma unroll
+  for (int a = 0; a < NA; ++a) {
+    const uint32_t k = t | (uint32_t(a) << bl);
+    double d = 0.0;
+    for (int s = 0; s < L; ++s) {
+      const double c = cb[3 * P + s];
+      d += ((k >> s) & 1u) ? c : -c;
+    }
+    for (int p = 0; p < P; ++p) {
+      const int2 q = pl[p];
+      const double c = cb[2 * P + p];
+      d += (((k >> q.x) ^ (k >> q.y)) & 1u) ? -c : c;
+    }
+    dg[a] = ty.scale * d;
+  }
+  __syncthreads();
+
+  const bool has_trans = (ty.flags & 1) != 0, has_fb = (ty.flags & 2) != 0;
+  const int ncorr = *sm.corr_n;
+  const double2* wts = args.wpool + ty.w_off;
+  const double a0 = wts[0].x;
+
+  for (int v = 0; v < 2; ++v) {
+    double2* psig = st + v * N;
+    double2 preg[PSI == PSI_REG ? NA : 1] = {};
+    // psi of amplitude slot a, wherever it lives
+    auto psi_ld = [&](int a) -> double2 {
+      const uint32_t k = t | (uint32_t(a) << bl);
+      if constexpr (PSI == PSI_REG) return preg[a];
+      else if constexpr (PSI == PSI_SMEM) return sm.psi[k];
+      else return __ldcg(&psig[k]);
+    };
+    auto psi_st = [&](int a, double2 p) {
+      const uint32_t k = t | (uint32_t(a) << bl);
+      if constexpr (PSI == PSI_REG) preg[a] = p;
+      else if constexpr (PSI == PSI_SMEM) sm.psi[k] = p;
+      else __stcg(&psig[k], p);
+    };
+    if constexpr (PSI != PSI_GLOBAL) {
+#pragma unroll
+      for (int a = 0; a < NA; ++a) {
+        const double2 p = psig[t | (uint32_t(a) << bl)];
+        if constexpr (PSI == PSI_REG) preg[a] = p;
+        else sm.psi[t | (uint32_t(a) << bl)] = p;
+      }
+    }
+    for (int step = 0; step < op.b; ++step) {
+      C2* cur = sm.buf[0];
+      C2* prv = sm.buf[1];
+      // T_0 = psi; psi *= a_0  (src/core/Propagator.cpp:53-55)
+#pragma unroll
+      for (int a = 0; a < NA; ++a) {
+        const uint32_t k = t | (uint32_t(a) << bl);
+        double2 p = psi_ld(a);
+        C2 c;
+        c.x = Real(p.x);
+        c.y = Real(p.y);
+        cur[pad<R>(k)] = c;
+        p.x *= a0;
+        p.y *= a0;
+        psi_st(a, p);
+      }
+      __syncthreads();
+      for (int n = 1; n <= ty.order; ++n) {
+        const double2 cn = wts[n];
+        front_layouts<L, R, Real, 0>(sm, cur, t, has_trans, has_fb);
+        C2 acc[NA], own[NA];
+        layout_pass<L, R, Real, G - 1>(sm, cur, acc, own, t, has_trans, has_fb);
+        C2* prv_mine = prv + pad<R>(t);  // last layout: pad(t | a << bl) = pad(t) + pad(a << bl)
+#pragma unroll
+        for (int a = 0; a < NA; ++a) {
+          const uint32_t k = t | (uint32_t(a) << bl);
+          // T_n in FP64: the FP32 partial sum, the FP64 diagonal, the FP64
+          // rounding residuals of the strongest couplings, the recurrence.
+          double hx = double(acc[a].x) + dg[a] * double(own[a].x);
+          double hy = double(acc[a].y) + dg[a] * double(own[a].y);
+#pragma unroll
+          for (int c = 0; c < kCorr; ++c) {
+            if (c < ncorr) {
+              const uint2 mk = sm.corr_mask[c];
+              const double2 cc = sm.corr_coef[c];
+              const C2 w = cur[pad<R>(k ^ mk.x ^ mk.y)];
+              const double co = (((k & mk.x) != 0) == ((k & mk.y) != 0)) ? cc.y : cc.x;
+              hx += co * double(w.x);
+              hy += co * double(w.y);
+            }
+          }
+          const uint32_t off = pad<R>(uint32_t(a) << bl);
+          if (n == 1) {
+            hx *= 0.5;
+            hy *= 0.5;
+          } else {
+            const C2 q = prv_mine[off];
+            hx -= double(q.x);
+            hy -= double(q.y);
+          }
+          C2 tn;
+          tn.x = Real(hx);
+          tn.y = Real(hy);
+          prv_mine[off] = tn;
+          double2 p = psi_ld(a);
+          p.x += cn.x * hx - cn.y * hy;
+          p.y += cn.x * hy + cn.y * hx;
+          psi_st(a, p);
+        }
+        __syncthreads();
+        C2* tmp = cur;
+        cur = prv;
+        prv = tmp;
+      }
+      if (op.c) {  // autonormalise (src/core/Propagator.cpp:98)
+        double s = 0.0;
+#pragma unroll
+        for (int a = 0; a < NA; ++a) {
+          const double2 p = psi_ld(a);
+          s += p.x * p.x + p.y * p.y;
+        }
+        const double nrm = sqrt(cta_sum2<NT>(make_double2(s, 0.0), sm.red).x);
+        if (nrm == 0.0 || !isfinite(nrm)) {
+          if (t == 0) atomicExch(args.flags, nrm == 0.0 ? SS_ERR_DOMAIN : SS_ERR_NUMERIC);
+        } else {
+          const double f = 1.0 / nrm;
+#pragma unroll
+          for (int a = 0; a < NA; ++a) {
+            double2 p = psi_ld(a);
+            p.x *= f;
+            p.y *= f;
+            psi_st(a, p);
+          }
+        }
+        __syncthreads();
+      }
+    }
+    if constexpr (PSI != PSI_GLOBAL) {
+#pragma unroll
+      for (int a = 0; a < NA; ++a) psig[t | (uint32_t(a) << bl)] = psi_ld(a);
+    }
+    __syncthreads();
+  }
+}
+
+template <int NT>
+__device__ void pulse_op(const Args& args, int L, double2* st, const Op& op) {
+  const double* u = args.rots + 8 * op.a;
+  const double llr = u[0], lli = u[1], lhr = u[2], lhi = u[3];
+  const double hlr = u[4], hli = u[5], hhr = u[6], hhi = u[7];
+  const uint32_t n = 1u << L;
+  const int s0 = op.b < 0 ? 0 : op.b, s1 = op.b < 0 ? L : op.b + 1;
+  for (int v = 0; v < 2; ++v) {
+    double2* psi = st + v * n;
+    for (int s = s0; s < s1; ++s) {
+      const uint32_t low = (1u << s) - 1u;
+      for (uint32_t j = threadIdx.x; j < n / 2; j += NT) {
+        const uint32_t lo = ((j & ~low) << 1) | (j & low);
+        const uint32_t hi = lo | (1u << s);
+        const double2 a = psi[lo], b = psi[hi];
+        psi[lo] = make_double2((llr * a.x - lli * a.y) + (lhr * b.x - lhi * b.y),
+                               (llr * a.y + lli * a.x) + (lhr * b.y + lhi * b.x));
+        psi[hi] = make_double2((hlr * a.x - hli * a.y) + (hhr * b.x - hhi * b.y),
+                               (hlr * a.y + hli * a.x) + (hhr * b.y + hhi * b.x));
+      }
+      __syncthreads();
+    }
+  }
+}
+
+template <int L, int NT>
+__device__ void measure_op(const Args& args, double2* stage, double2* red, const RealDev& rd,
+                           const double2* st, const Op& op) {
+  constexpr uint32_t N = 1u << L;
+  const uint32_t t = threadIdx.x;
+  __syncthreads();
+  for (uint32_t k = t; k < N; k += NT) stage[k] = st[k];
+  __syncthreads();
+  const double2* ref = st + N;
+  double* row = args.rows + rd.row_off + static_cast<long long>(op.a) * args.width;
+  int col = 0;
+  for (int i = 0; i < args.nobs; ++i) {
+    const int kind = args.obs[3 * i], axis = args.obs[3 * i + 1], spin = args.obs[3 * i + 2];
+    double2 v = make_double2(0.0, 0.0);
+    if (kind == SS_OBS_CORR) {
+      for (uint32_t k = t; k < N; k += NT) {
+        double sr = 0.0, si = 0.0;
+        for (int s = 0; s < L; ++s) {
+          const double2 q = sigma_at(stage, k, s, axis);
+          sr += q.x;
+          si += q.y;
+        }
+        const double2 r = ref[k];
+        v.x += r.x * sr + r.y * si;
+        v.y += r.x * si - r.y * sr;
+      }
+    } else if (kind == SS_OBS_MAG) {
+      for (uint32_t k = t; k < N; k += NT) {
+        const double2 q = sigma_at(stage, k, spin, axis);
+        const double2 p = stage[k];
+        v.x += p.x * q.x + p.y * q.y;
+      }
+    } else if (kind == SS_OBS_NORM) {
+      for (uint32_t k = t; k < N; k += NT) {
+        const double2 p = stage[k], r = ref[k];
+        v.x += p.x * p.x + p.y * p.y;
+        v.y += r.x * r.x + r.y * r.y;
+      }
+    } else {  // energy with the realisation's own fields, FP64
+      const TypeDev ty = args.types[rd.type_off + args.measure_type];
+      const double* cb = args.cpool + ty.c_off;
+      const int2* pl = args.pairs + rd.pair_off;
+      const int P = rd.npairs;
+      for (uint32_t k = t; k < N; k += NT) {
+        const double2 p = stage[k];
+        double d = 0.0;
+        for (int s = 0; s < L; ++s) d += ((k >> s) & 1u) ? cb[3 * P + s] : -cb[3 * P + s];
+        for (int q = 0; q < P; ++q) {
+          const int2 pr = pl[q];
+          d += (((k >> pr.x) ^ (k >> pr.y)) & 1u) ? -cb[2 * P + q] : cb[2 * P + q];
+        }
+        double hr = d * p.x, hi = d * p.y;
+        for (int s = 0; s < L; ++s) {
+          const double cx = cb[3 * P + L + s];
+          const double cy = ((k >> s) & 1u) ? -cb[3 * P + 2 * L + s] : cb[3 * P + 2 * L + s];
+          const double2 w = stage[k ^ (1u << s)];
+          hr += cx * w.x - cy * w.y;
+          hi += cx * w.y + cy * w.x;
+        }
+        for (int q = 0; q < P; ++q) {
+          const int2 pr = pl[q];
+          const bool anti = (((k >> pr.x) ^ (k >> pr.y)) & 1u) != 0;
+          const double c = anti ? cb[q] : cb[P + q];
+          const double2 w = stage[k ^ (1u << pr.x) ^ (1u << pr.y)];
+          hr += c * w.x;
+          hi += c * w.y;
+        }
+        v.x += hr * p.x + hi * p.y;
+      }
+    }
+    v = cta_sum2<NT>(v, red);
+    if (t == 0) {
+      if (kind == SS_OBS_CORR) {
+        row[col] = v.x;
+        row[col + 1] = v.y;
+      } else if (kind == SS_OBS_NORM) {
+        row[col] = sqrt(v.x);
+        row[col + 1] = sqrt(v.y);
+      } else {
+        row[col] = v.x;
+      }
+    }
+    col += (kind == SS_OBS_CORR || kind == SS_OBS_NORM) ? 2 : 1;
+  }
+  __syncthreads();
+}
+
+// Shared-memory carve-up: three recursion buffers, psi (when it lives here),
+// the coupling tables, the correction terms and the reduction slots.
+template <int L, int R, typename Real, int PSI>
+struct SmemLayout {
+  using C2 = typename Cplx<Real>::T;
+  static constexpr size_t N = size_t{1} << L;
+  static constexpr size_t NP = (size_t{1} << L) + (size_t{1} << (L - R));  // padded
+  static constexpr size_t bufs = 3 * NP * sizeof(C2);
+  static constexpr size_t psi = PSI == PSI_SMEM ? N * sizeof(double2) : 0;
+  static constexpr size_t at_psi = bufs;
+  static constexpr size_t at_coef = at_psi + psi;
+  static constexpr size_t coef = (2 * L * L + 2 * L) * sizeof(Real);
+  static constexpr size_t at_corr = (at_coef + coef + 15) & ~size_t{15};
+  static constexpr size_t corr = kCorr * (sizeof(uint2) + sizeof(double2)) + 16;
+  static constexpr size_t at_red = (at_corr + corr + 15) & ~size_t{15};
+  static constexpr size_t total = at_red + 32 * sizeof(double2);
+};
+
+template <int L, int R, typename Real, int PSI>
+__global__ void __launch_bounds__(Geo<L, R>::NT) k_batch(const __grid_constant__ Args args) {
+  using Gm = Geo<L, R>;
+  using C2 = typename Cplx<Real>::T;
+  using SL = SmemLayout<L, R, Real, PSI>;
+  constexpr int NT = Gm::NT, N = static_cast<int>(SL::NP);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Smem<Real> sm;
+  C2* base = reinterpret_cast<C2*>(smem_raw);
+  sm.buf[0] = base;
+  sm.buf[1] = base + N;
+  sm.buf[2] = base + 2 * N;
+  sm.psi = reinterpret_cast<double2*>(smem_raw + SL::at_psi);
+  Real* coef = reinterpret_cast<Real*>(smem_raw + SL::at_coef);
+  sm.cff = coef;
+  sm.cfb = coef + L * L;
+  sm.ccx = coef + 2 * L * L;
+  sm.ccy = coef + 2 * L * L + L;
+  sm.corr_coef = reinterpret_cast<double2*>(smem_raw + SL::at_corr);
+  sm.corr_mask = reinterpret_cast<uint2*>(smem_raw + SL::at_corr + kCorr * sizeof(double2));
+  sm.corr_n = reinterpret_cast<int*>(smem_raw + SL::at_corr + kCorr * (sizeof(double2) + sizeof(uint2)));
+  sm.red = reinterpret_cast<double2*>(smem_raw + SL::at_red);
+  __shared__ int s_work;
+
+  for (;;) {
+    if (threadIdx.x == 0) s_work = static_cast<int>(atomicAdd(args.counter, 1u));
+    __syncthreads();
+    const int w = s_work;
+    __syncthreads();
+    if (w >= args.nwork) break;
+    const RealDev rd = args.reals[args.work[w]];
+    double2* st = args.states + rd.state_off;
+    for (int i = args.op_begin; i < args.op_end; ++i) {
+      const Op op = args.ops[i];
+      if (op.kind == OP_EVOLVE) {
+        const TypeDev ty = args.types[rd.type_off + op.a];
+        if (ty.order > 0 && op.b > 0) evolve_op<L, R, Real, PSI>(args, sm, rd, st, op, ty);
+      } else if (op.kind == OP_PULSE) {
+        pulse_op<NT>(args, L, st, op);
+      } else {
+        measure_op<L, NT>(args, reinterpret_cast<double2*>(smem_raw), sm.red, rd, st, op);
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------ variants
+struct Variant {
+  int L, R;
+  bool mixed;
+  int psi;
+  int threads;
+  size_t smem;
+  void (*kernel)(Args);
+};
+
+template <int L, int R, typename Real, int PSI>
+Variant make_variant() {
+  return Variant{L, R, std::is_same<Real, float>::value, PSI, Geo<L, R>::NT,
+                 SmemLayout<L, R, Real, PSI>::total, &k_batch<L, R, Real, PSI>};
+}
+
+// The per-size schedules: register bits R and where psi lives.  Chosen so a
+// realisation fits one CTA (threads = 2^(L-R) >= 32), the three shared
+// buffers fit 227 KB, and the registers fit the thread count.
+const std::vector<Variant>& variants() {
+  static const std::vector<Variant> v = {
+      make_variant<6, 1, float, PSI_REG>(),     make_variant<7, 2, float, PSI_REG>(),
+      make_variant<8, 3, float, PSI_REG>(),     make_variant<9, 4, float, PSI_SMEM>(),
+      make_variant<10, 4, float, PSI_SMEM>(),   make_variant<11, 4, float, PSI_SMEM>(),
+      make_variant<12, 4, float, PSI_SMEM>(),   make_variant<13, 4, float, PSI_GLOBAL>(),
+      make_variant<6, 1, double, PSI_REG>(),    make_variant<7, 2, double, PSI_REG>(),
+      make_variant<8, 3, double, PSI_REG>(),    make_variant<9, 3, double, PSI_SMEM>(),
+      make_variant<10, 3, double, PSI_SMEM>(),  make_variant<11, 3, double, PSI_SMEM>(),
+      make_variant<12, 3, double, PSI_GLOBAL>(),
+  };
+  return v;
+}
+
+const Variant* find_variant(int L, bool mixed) {
+  for (const Variant& v : variants()) {
+    if (v.L == L && v.mixed == mixed) return &v;
+  }
+  return nullptr;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ host
+struct TypeKey {
+  int table;
+  int from_draw;
+  int mode;
+  double tau;
+  bool operator<(const TypeKey& o) const {
+    return std::tie(table, from_draw, mode, tau) < std::tie(o.table, o.from_draw, o.mode, o.tau);
+  }
+};
+
+struct Bucket {
+  int L = 0;
+  const Variant* var = nullptr;
+  std::vector<int> work;
+  int grid = 0;
+  unsigned int* counter = nullptr;
+  int* dev_work = nullptr;
+  cudaStream_t side = nullptr;
+};
+
+}  // namespace batch
+}  // namespace ss
+
+using namespace ss;
+using namespace ss::batch;
+
+struct ss_batch {
+  ss_engine* engine = nullptr;
+  int precision = SS_PRECISION_MIXED;
+  uint64_t first = 0;
+  int64_t count = 0;
+  int64_t points = 0, width = 0;
+  int ntypes = 0;  // evolve step types; slot ntypes is the energy table
+  std::vector<double> times;
+  // host staging
+  std::vector<Op> ops;
+  std::vector<double> rots;
+  std::vector<RealDev> reals;
+  std::vector<TypeDev> types;
+  std::vector<double> cpool;
+  std::vector<double> wpool;  // (re, im) pairs
+  std::vector<int2> pairs;
+  std::vector<double> psi0;   // (re, im) pairs
+  std::vector<long long> psi0_off;
+  std::vector<int> obs;
+  std::vector<Bucket> buckets;
+  int ref_axis = 0;
+  long long state_len = 0, rows_len = 0;
+  int64_t orders_total = 0;
+  double amp_orders = 0.0;
+  int64_t launches_per_run = 0;
+  // device
+  Op* d_ops = nullptr;
+  double* d_rots = nullptr;
+  RealDev* d_reals = nullptr;
+  TypeDev* d_types = nullptr;
+  double* d_cpool = nullptr;
+  double2* d_wpool = nullptr;
+  int2* d_pairs = nullptr;
+  double2* d_psi0 = nullptr;
+  long long* d_psi0_off = nullptr;
+  double2* d_states = nullptr;
+  double* d_rows = nullptr;
+  int* d_obs = nullptr;
+  int* d_flags = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  bool uploaded = false;
+};
+
+namespace ss {
+namespace batch {
+namespace {
+
+template <typename T>
+void dev_alloc(T** p, size_t n) {
+  SS_CUDA(cudaMalloc(reinterpret_cast<void**>(p), sizeof(T) * std::max<size_t>(n, 1)));
+}
+
+template <typename T>
+void upload_vec(T* dst, const std::vector<T>& src, cudaStream_t s) {
+  if (!src.empty()) {
+    SS_CUDA(cudaMemcpyAsync(dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice, s));
+  }
+}
+
+void linearise(const ss_run_config& c, int begin, int end, std::vector<Op>& ops,
+               std::map<TypeKey, int>& types, std::vector<TypeKey>& keys,
+               std::map<std::vector<double>, int>& rot_ids, std::vector<double>& rots,
+               int64_t& point) {
+  for (int at = begin; at < end;) {
+    const ss_step& s = c.steps[at];
+    if (s.kind == SS_STEP_EVOLVE) {
+      const TypeKey key{s.field_table, s.tau_from_draw ? 1 : 0, s.mode, s.tau};
+      auto it = types.find(key);
+      if (it == types.end()) {
+        it = types.emplace(key, static_cast<int>(keys.size())).first;
+        keys.push_back(key);
+      }
+      require(s.count >= 0 && s.count < (int64_t{1} << 30), SS_ERR_CONFIG, "step count out of range");
+      ops.push_back(Op{OP_EVOLVE, it->second, static_cast<int>(s.count), s.autonormalize ? 1 : 0});
+      ++at;
+    } else if (s.kind == SS_STEP_PULSE) {
+      double u[8];
+      rotation_matrix(s.axis, s.angle, u);
+      std::vector<double> key(u, u + 8);
+      auto it = rot_ids.find(key);
+      if (it == rot_ids.end()) {
+        it = rot_ids.emplace(key, static_cast<int>(rots.size() / 8)).first;
+        rots.insert(rots.end(), u, u + 8);
+      }
+      ops.push_back(Op{OP_PULSE, it->second, s.target, 0});
+      ++at;
+    } else if (s.kind == SS_STEP_MEASURE) {
+      ops.push_back(Op{OP_MEASURE, static_cast<int>(point++), 0, 0});
+      ++at;
+    } else {
+      for (int64_t i = 0; i < s.count; ++i) {
+        linearise(c, at + 1, at + 1 + s.body_len, ops, types, keys, rot_ids, rots, point);
+      }
+      at += 1 + s.body_len;
+    }
+  }
+}
+
+// Coefficient block of one table (see TypeDev) with the reference's skip rule.
+void coefficient_block(int L, const double* f, const std::vector<PairTerm>& pairs, double scale,
+                       std::vector<double>& out, int* flags) {
+  const size_t P = pairs.size();
+  const size_t at = out.size();
+  out.resize(at + 3 * P + 3 * L + 4 * kCorr, 0.0);
+  double* cb = out.data() + at;
+  for (size_t p = 0; p < P; ++p) {
+    const double q = scale * 0.25;
+    const double ff = q * (pairs[p].jx + pairs[p].jy);
+    const double fb = q * (pairs[p].jx - pairs[p].jy);
+    if (std::abs(ff) > kNegligible) cb[p] = ff;
+    if (std::abs(fb) > kNegligible) {
+      cb[P + p] = fb;
+      *flags |= 2;
+    }
+    const double z = 0.25 * pairs[p].jz;
+    if (std::abs(z) > kNegligible) cb[2 * P + p] = z;
+  }
+  for (int s = 0; s < L; ++s) {
+    const double z = 0.5 * f[3 * s + 2];
+    if (std::abs(z) > kNegligible) cb[3 * P + s] = z;
+    const double cx = scale * 0.5 * f[3 * s], cy = scale * 0.5 * f[3 * s + 1];
+    if (std::abs(cx) > kNegligible || std::abs(cy) > kNegligible) {
+      cb[3 * P + L + s] = cx;
+      cb[3 * P + 2 * L + s] = cy;
+      *flags |= 1;
+    }
+  }
+  // The kCorr strongest couplings and their FP32 rounding residuals.
+  std::vector<size_t> idx(P);
+  std::iota(idx.begin(), idx.end(), size_t{0});
+  std::stable_sort(idx.begin(), idx.end(), [&](size_t x, size_t y) {
+    return std::abs(cb[x]) + std::abs(cb[P + x]) > std::abs(cb[y]) + std::abs(cb[P + y]);
+  });
+  double* ct = cb + 3 * P + 3 * L;
+  for (int c = 0; c < kCorr; ++c) {
+    ct[4 * c] = -1.0;
+    if (static_cast<size_t>(c) >= P) continue;
+    const size_t p = idx[static_cast<size_t>(c)];
+    const double rff = cb[p] - static_cast<double>(static_cast<float>(cb[p]));
+    const double rfb = cb[P + p] - static_cast<double>(static_cast<float>(cb[P + p]));
+    if (rff == 0.0 && rfb == 0.0) continue;
+    ct[4 * c] = static_cast<double>(p);
+    ct[4 * c + 1] = rff;
+    ct[4 * c + 2] = rfb;
+  }
+}
+
+struct PerReal {
+  int L = 0;
+  double tau_draw = 1.0;
+  std::vector<int2> pairs;
+  std::vector<double> psi0;
+  std::vector<TypeDev> types;
+  std::vector<double> cpool, wpool;
+  double cost = 0.0;
+  int64_t orders = 0;
+  double amp_orders = 0.0;
+  int error = 0;
+  std::string message;
+};
+
+// Mixed precision applies a pulse's transverse field as one FP32 number per
+// spin; its rounding is a coherent flip-angle error repeated at every pulse.
+// When the field is uniform (the same hx, or the same hy, on every spin) the
+// expansion is rebuilt on a normalisation bound' within 1e-7 of the bound,
+// chosen so that the scaled field is exactly an FP32 number.  Any bound' at
+// least ||H|| gives the same propagator (the sum of term norms overestimates
+// ||H|| by percents), and the truncation order is kept, so the FP64 result is
+// unchanged to the level of the truncated tail.
+void exact_transverse(int L, const double* f, int mode, double tau, Expansion& ex) {
+  if (ex.order() == 0) return;
+  const double hx = f[0], hy = f[1];
+  if ((hx == 0.0) == (hy == 0.0)) return;  // none, or both components
+  for (int s = 1; s < L; ++s) {
+    if (f[3 * s] != hx || f[3 * s + 1] != hy) return;
+  }
+  const double h = hx != 0.0 ? hx : hy;
+  const double scale = -2.0 / ex.bound;
+  const double c32 = static_cast<double>(static_cast<float>(scale * 0.5 * h));
+  const double scale2 = c32 / (0.5 * h);
+  const double c2 = scale2 * 0.5 * h;
+  if (!(scale2 < 0.0) || c2 != static_cast<double>(static_cast<float>(c2))) return;
+  const double bound2 = -2.0 / scale2;
+  if (std::abs(bound2 - ex.bound) > 1e-7 * ex.bound) return;
+  const size_t order = ex.order();
+  std::vector<double> a = bessel(mode == SS_TIME_IMAGINARY ? 1 : 0, bound2 * std::abs(tau),
+                                 order + 1, nullptr);
+  if (tau < 0.0) {
+    for (size_t n = 1; n < a.size(); n += 2) a[n] = -a[n];
+  }
+  ex.a = a;
+  ex.bound = bound2;
+}
+
+void build_realization(const ss_run_config& c, uint64_t index, const std::vector<TypeKey>& keys,
+                       const std::vector<Op>& ops, bool mixed, PerReal& out) {
+  try {
+    const Realization rz = assemble_realization(c, index);
+    out.L = rz.nspins;
+    out.tau_draw = rz.tau_draw;
+    out.psi0 = rz.psi0;
+    for (const PairTerm& p : rz.pairs) out.pairs.push_back(make_int2(p.lo, p.hi));
+    const int L = rz.nspins;
+    std::vector<int> orders(keys.size(), 0);
+    for (size_t t = 0; t < keys.size(); ++t) {
+      const TypeKey& k = keys[t];
+      const double* f = k.table >= 0 ? c.step_fields + static_cast<size_t>(3) * c.nspins * k.table
+                                     : rz.fields.data();
+      const double tau = k.from_draw ? k.tau * rz.tau_draw : k.tau;
+      Expansion ex = chebyshev(k.mode, spectral_bound(L, f, rz.pairs), tau, c.epsilon);
+      if (mixed) exact_transverse(L, f, k.mode, tau, ex);
+      TypeDev ty{};
+      ty.order = static_cast<int>(ex.order());
+      orders[t] = ty.order;
+      ty.c_off = static_cast<long long>(out.cpool.size());
+      if (ty.order > 0) {
+        ty.scale = -2.0 / ex.bound;
+        ty.w_off = static_cast<long long>(out.wpool.size() / 2);
+        const std::vector<double> w = series_weights(ex, k.mode);
+        out.wpool.insert(out.wpool.end(), w.begin(), w.end());
+        coefficient_block(L, f, rz.pairs, ty.scale, out.cpool, &ty.flags);
+      }
+      out.types.push_back(ty);
+    }
+    TypeDev energy{};
+    energy.scale = 1.0;
+    energy.c_off = static_cast<long long>(out.cpool.size());
+    coefficient_block(L, rz.fields.data(), rz.pairs, 1.0, out.cpool, &energy.flags);
+    out.types.push_back(energy);
+    for (const Op& op : ops) {
+      if (op.kind == OP_EVOLVE) {
+        const double work = static_cast<double>(orders[op.a]) * op.b;
+        out.orders += 2 * static_cast<int64_t>(orders[op.a]) * op.b;
+        out.amp_orders += 2.0 * work * static_cast<double>(size_t{1} << L);
+      }
+    }
+    out.cost = out.amp_orders + 64.0 * static_cast<double>(size_t{1} << L);
+  } catch (const Error& e) {
+    out.error = e.code;
+    out.message = e.what();
+  } catch (const std::exception& e) {
+    out.error = SS_ERR_RUNTIME;
+    out.message = e.what();
+  }
+}
+
+void build_plan(ss_batch* b, const ss_run_config& c) {
+  validate_config(c);
+  std::map<TypeKey, int> type_ids;
+  std::vector<TypeKey> keys;
+  std::map<std::vector<double>, int> rot_ids;
+  int64_t point = 0;
+  linearise(c, 0, c.n_steps, b->ops, type_ids, keys, rot_ids, b->rots, point);
+  b->points = point;
+  b->width = observable_width(c.observables, c.n_observables);
+  b->ntypes = static_cast<int>(keys.size());
+  b->ref_axis = c.reference_axis;
+  for (int i = 0; i < c.n_observables; ++i) {
+    const ss_observable& o = c.observables[i];
+    require(o.kind >= 0 && o.kind <= 3, SS_ERR_CONFIG, "unknown observable");
+    require(o.axis >= 0 && o.axis <= 2, SS_ERR_CONFIG, "unknown axis; expected x, y or z");
+    b->obs.insert(b->obs.end(), {o.kind, o.axis, o.spin});
+  }
+  for (const Op& op : b->ops) {
+    if (op.kind == OP_PULSE) {
+      require(op.b < c.nspins, SS_ERR_OUT_OF_RANGE, "rotation names a spin outside the system");
+    }
+  }
+
+  std::vector<PerReal> per(static_cast<size_t>(b->count));
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t workers = std::min<size_t>(hw, per.size());
+  {
+    std::vector<std::thread> pool;
+    std::atomic<size_t> next{0};
+    for (size_t w = 0; w < workers; ++w) {
+      pool.emplace_back([&] {
+        for (size_t i = next.fetch_add(1); i < per.size(); i = next.fetch_add(1)) {
+          build_realization(c, b->first + i, keys, b->ops, b->precision == SS_PRECISION_MIXED,
+                            per[i]);
+        }
+      });
+    }
+    for (auto& th : pool) th.join();
+  }
+  for (const PerReal& pr : per) {
+    if (pr.error) fail(pr.error, pr.message);
+  }
+
+  long long state_off = 0, row_off = 0;
+  std::map<int, std::vector<int>> by_size;
+  for (size_t i = 0; i < per.size(); ++i) {
+    PerReal& pr = per[i];
+    for (int o = 0; o < c.n_observables; ++o) {
+      if (c.observables[o].kind == SS_OBS_MAG) {
+        require(c.observables[o].spin >= 0 && c.observables[o].spin < pr.L, SS_ERR_OUT_OF_RANGE,
+                "observable names a spin outside the system");
+      }
+    }
+    RealDev rd{};
+    rd.L = pr.L;
+    rd.npairs = static_cast<int>(pr.pairs.size());
+    rd.pair_off = static_cast<long long>(b->pairs.size());
+    rd.state_off = state_off;
+    rd.type_off = static_cast<long long>(b->types.size());
+    rd.row_off = row_off;
+    const long long c_base = static_cast<long long>(b->cpool.size());
+    const long long w_base = static_cast<long long>(b->wpool.size() / 2);
+    for (TypeDev ty : pr.types) {
+      ty.c_off += c_base;
+      ty.w_off += w_base;
+      b->types.push_back(ty);
+    }
+    b->pairs.insert(b->pairs.end(), pr.pairs.begin(), pr.pairs.end());
+    b->cpool.insert(b->cpool.end(), pr.cpool.begin(), pr.cpool.end());
+    b->wpool.insert(b->wpool.end(), pr.wpool.begin(), pr.wpool.end());
+    b->psi0_off.push_back(static_cast<long long>(b->psi0.size() / 2));
+    b->psi0.insert(b->psi0.end(), pr.psi0.begin(), pr.psi0.end());
+    b->reals.push_back(rd);
+    state_off += 2LL << pr.L;
+    row_off += b->points * b->width;
+    b->orders_total += pr.orders;
+    b->amp_orders += pr.amp_orders;
+    by_size[pr.L].push_back(static_cast<int>(i));
+  }
+  b->state_len = state_off;
+  b->rows_len = row_off;
+
+  // Times of the first realisation (the reference reports the first's,
+  // src/ensemble/EnsembleRunner.cpp:72).
+  {
+    double time = 0.0;
+    for (const Op& op : b->ops) {
+      if (op.kind == OP_EVOLVE) {
+        const TypeKey& k = keys[op.a];
+        const double tau = k.from_draw ? k.tau * per.front().tau_draw : k.tau;
+        time += tau * static_cast<double>(op.b);
+      } else if (op.kind == OP_MEASURE) {
+        b->times.push_back(time);
+      }
+    }
+  }
+
+  const bool mixed = b->precision == SS_PRECISION_MIXED;
+  ss_engine* e = b->engine;
+  for (auto& [L, list] : by_size) {
+    Bucket bk;
+    bk.L = L;
+    bk.var = find_variant(L, mixed);
+    if (!bk.var) {
+      fail(SS_ERR_INVALID_ARGUMENT,
+           std::string("the batched engine covers L = 6..") + (mixed ? "13" : "12") +
+               " in this precision; got L = " + std::to_string(L));
+    }
+    std::stable_sort(list.begin(), list.end(),
+                     [&](int x, int y) { return per[x].cost > per[y].cost; });
+    bk.work = list;
+    SS_CUDA(cudaFuncSetAttribute(bk.var->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(bk.var->smem)));
+    int per_sm = 0;
+    SS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bk.var->kernel,
+                                                          bk.var->threads, bk.var->smem));
+    require(per_sm > 0, SS_ERR_RUNTIME, "batched kernel does not fit an SM");
+    bk.grid = std::min<int>(per_sm * e->sm_count, static_cast<int>(list.size()));
+    b->buckets.push_back(std::move(bk));
+  }
+}
+
+void capture(ss_batch* b) {
+  ss_engine* e = b->engine;
+  cudaStream_t s = e->stream;
+  SS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  try {
+    SS_CUDA(cudaMemsetAsync(b->d_flags, 0, sizeof(int), s));
+    k_batch_prepare<<<static_cast<unsigned>(b->count), kPrepThreads, 0, s>>>(
+        b->d_reals, b->d_psi0, b->d_psi0_off, b->d_states, b->ref_axis);
+    SS_CUDA(cudaGetLastError());
+    int64_t launches = 1;
+    std::vector<cudaEvent_t> joins;
+    cudaEvent_t fork;
+    SS_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    SS_CUDA(cudaEventRecord(fork, s));
+    for (size_t i = 0; i < b->buckets.size(); ++i) {
+      Bucket& bk = b->buckets[i];
+      cudaStream_t ks = s;
+      if (i > 0) {
+        ks = bk.side;
+        SS_CUDA(cudaStreamWaitEvent(ks, fork, 0));
+      }
+      SS_CUDA(cudaMemsetAsync(bk.counter, 0, sizeof(unsigned int), ks));
+      Args a{};
+      a.ops = b->d_ops;
+      a.op_begin = 0;
+      a.op_end = static_cast<int>(b->ops.size());
+      a.rots = b->d_rots;
+      a.reals = b->d_reals;
+      a.work = bk.dev_work;
+      a.nwork = static_cast<int>(bk.work.size());
+      a.counter = bk.counter;
+      a.types = b->d_types;
+      a.cpool = b->d_cpool;
+      a.wpool = b->d_wpool;
+      a.pairs = b->d_pairs;
+      a.states = b->d_states;
+      a.rows = b->d_rows;
+      a.obs = b->d_obs;
+      a.nobs = static_cast<int>(b->obs.size() / 3);
+      a.width = static_cast<int>(b->width);
+      a.measure_type = b->ntypes;
+      a.flags = b->d_flags;
+      bk.var->kernel<<<bk.grid, bk.var->threads, bk.var->smem, ks>>>(a);
+      SS_CUDA(cudaGetLastError());
+      ++launches;
+      if (i > 0) {
+        cudaEvent_t j;
+        SS_CUDA(cudaEventCreateWithFlags(&j, cudaEventDisableTiming));
+        SS_CUDA(cudaEventRecord(j, ks));
+        joins.push_back(j);
+      }
+    }
+    for (cudaEvent_t j : joins) SS_CUDA(cudaStreamWaitEvent(s, j, 0));
+    SS_CUDA(cudaStreamEndCapture(s, &b->graph));
+    cudaEventDestroy(fork);
+    for (cudaEvent_t j : joins) cudaEventDestroy(j);
+    b->launches_per_run = launches;
+  } catch (...) {
+    cudaGraph_t g = nullptr;
+    cudaStreamEndCapture(s, &g);
+    if (g) cudaGraphDestroy(g);
+    throw;
+  }
+  SS_CUDA(cudaGraphInstantiate(&b->exec, b->graph, 0));
+}
+
+void upload(ss_batch* b) {
+  cudaStream_t s = b->engine->stream;
+  upload_vec(b->d_ops, b->ops, s);
+  upload_vec(b->d_rots, b->rots, s);
+  upload_vec(b->d_reals, b->reals, s);
+  upload_vec(b->d_types, b->types, s);
+  upload_vec(b->d_cpool, b->cpool, s);
+  if (!b->wpool.empty()) {
+    SS_CUDA(cudaMemcpyAsync(b->d_wpool, b->wpool.data(), sizeof(double) * b->wpool.size(),
+                            cudaMemcpyHostToDevice, s));
+  }
+  upload_vec(b->d_pairs, b->pairs, s);
+  SS_CUDA(cudaMemcpyAsync(b->d_psi0, b->psi0.data(), sizeof(double) * b->psi0.size(),
+                          cudaMemcpyHostToDevice, s));
+  upload_vec(b->d_psi0_off, b->psi0_off, s);
+  upload_vec(b->d_obs, b->obs, s);
+  for (Bucket& bk : b->buckets) upload_vec(bk.dev_work, bk.work, s);
+  sync(b->engine);
+  b->uploaded = true;
+}
+
+void execute(ss_batch* b) {
+  require(b->uploaded, SS_ERR_RUNTIME, "batch inputs were not uploaded");
+  if (!b->exec) capture(b);
+  SS_CUDA(cudaGraphLaunch(b->exec, b->engine->stream));
+  b->engine->launches.fetch_add(b->launches_per_run, std::memory_order_relaxed);
+}
+
+void download(ss_batch* b, double* rows, double* times) {
+  ss_engine* e = b->engine;
+  int flag = 0;
+  SS_CUDA(cudaMemcpyAsync(&flag, b->d_flags, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+  if (rows) {
+    SS_CUDA(cudaMemcpyAsync(rows, b->d_rows, sizeof(double) * b->rows_len,
+                            cudaMemcpyDeviceToHost, e->stream));
+  }
+  sync(e);
+  if (flag == SS_ERR_DOMAIN) fail(flag, "cannot normalize a zero state");
+  if (flag) fail(flag, "a norm reduction saw NaN or Inf");
+  if (times) std::copy(b->times.begin(), b->times.end(), times);
+}
+
+void release(ss_batch* b) {
+  if (b->engine && b->engine->stream) cudaStreamSynchronize(b->engine->stream);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  cudaFree(b->d_ops);
+  cudaFree(b->d_rots);
+  cudaFree(b->d_reals);
+  cudaFree(b->d_types);
+  cudaFree(b->d_cpool);
+  cudaFree(b->d_wpool);
+  cudaFree(b->d_pairs);
+  cudaFree(b->d_psi0);
+  cudaFree(b->d_psi0_off);
+  cudaFree(b->d_states);
+  cudaFree(b->d_rows);
+  cudaFree(b->d_obs);
+  cudaFree(b->d_flags);
+  for (Bucket& bk : b->buckets) {
+    cudaFree(bk.counter);
+    cudaFree(bk.dev_work);
+    if (bk.side) cudaStreamDestroy(bk.side);
+  }
+}
+
+}  // namespace
+}  // namespace batch
+}  // namespace ss
+
+extern "C" {
+
+int ss_batch_create(ss_engine* engine, const ss_run_config* config, uint64_t first, int64_t count,
+                    int precision, ss_batch** out) {
+  return guarded([&] {
+    require(engine != nullptr && config != nullptr && out != nullptr, SS_ERR_INVALID_ARGUMENT,
+            "null argument");
+    require(count >= 1, SS_ERR_INVALID_ARGUMENT, "an ensemble needs at least one realisation");
+    require(precision == SS_PRECISION_FP64 || precision == SS_PRECISION_MIXED,
+            SS_ERR_INVALID_ARGUMENT, "unknown precision");
+    auto* b = new ss_batch;
+    b->engine = engine;
+    b->precision = precision;
+    b->first = first;
+    b->count = count;
+    try {
+      SS_CUDA(cudaSetDevice(engine->device));
+      build_plan(b, *config);
+      dev_alloc(&b->d_ops, b->ops.size());
+      dev_alloc(&b->d_rots, b->rots.size());
+      dev_alloc(&b->d_reals, b->reals.size());
+      dev_alloc(&b->d_types, b->types.size());
+      dev_alloc(&b->d_cpool, b->cpool.size());
+      dev_alloc(&b->d_wpool, b->wpool.size() / 2);
+      dev_alloc(&b->d_pairs, b->pairs.size());
+      dev_alloc(&b->d_psi0, b->psi0.size() / 2);
+      dev_alloc(&b->d_psi0_off, b->psi0_off.size());
+      dev_alloc(&b->d_states, static_cast<size_t>(b->state_len));
+      dev_alloc(&b->d_rows, static_cast<size_t>(b->rows_len));
+      dev_alloc(&b->d_obs, b->obs.size());
+      dev_alloc(&b->d_flags, 1);
+      for (Bucket& bk : b->buckets) {
+        dev_alloc(&bk.counter, 1);
+        dev_alloc(&bk.dev_work, bk.work.size());
+        SS_CUDA(cudaStreamCreateWithFlags(&bk.side, cudaStreamNonBlocking));
+      }
+    } catch (...) {
+      release(b);
+      delete b;
+      throw;
+    }
+    *out = b;
+  });
+}
+
+int ss_batch_destroy(ss_batch* b) {
+  return guarded([&] {
+    if (!b) return;
+    release(b);
+    delete b;
+  });
+}
+
+int ss_batch_shape(const ss_batch* b, int64_t* points, int64_t* width) {
+  return guarded([&] {
+    require(b != nullptr, SS_ERR_INVALID_ARGUMENT, "null batch");
+    if (points) *points = b->points;
+    if (width) *width = b->width;
+  });
+}
+
+int ss_batch_upload(ss_batch* b) {
+  return guarded([&] {
+    require(b != nullptr, SS_ERR_INVALID_ARGUMENT, "null batch");
+    upload(b);
+  });
+}
+
+int ss_batch_execute(ss_batch* b) {
+  return guarded([&] {
+    require(b != nullptr, SS_ERR_INVALID_ARGUMENT, "null batch");
+    execute(b);
+  });
+}
+
+int ss_batch_download(ss_batch* b, double* rows, double* times) {
+  return guarded([&] {
+    require(b != nullptr, SS_ERR_INVALID_ARGUMENT, "null batch");
+    download(b, rows, times);
+  });
+}
+
+int ss_batch_run(ss_batch* b, double* rows, double* times) {
+  return guarded([&] {
+    require(b != nullptr, SS_ERR_INVALID_ARGUMENT, "null batch");
+    upload(b);
+    execute(b);
+    download(b, rows, times);
+  });
+}
+
+int ss_batch_stats(const ss_batch* b, int64_t* orders, double* amplitude_orders,
+                   int64_t* launches) {
+  return guarded([&] {
+    require(b != nullptr, SS_ERR_INVALID_ARGUMENT, "null batch");
+    if (orders) *orders = b->orders_total;
+    if (amplitude_orders) *amplitude_orders = b->amp_orders;
+    if (launches) *launches = b->launches_per_run > 0 ? b->launches_per_run
+                                                      : 1 + static_cast<int64_t>(b->buckets.size());
+  });
+}
+
+int ss_batch_io_bytes(const ss_batch* b, int64_t* h2d, int64_t* d2h) {
+  return guarded([&] {
+    require(b != nullptr, SS_ERR_INVALID_ARGUMENT, "null batch");
+    int64_t in = 0;
+    in += static_cast<int64_t>(sizeof(Op) * b->ops.size() + sizeof(double) * b->rots.size());
+    in += static_cast<int64_t>(sizeof(RealDev) * b->reals.size() + sizeof(TypeDev) * b->types.size());
+    in += static_cast<int64_t>(sizeof(double) * (b->cpool.size() + b->wpool.size() + b->psi0.size()));
+    in += static_cast<int64_t>(sizeof(int2) * b->pairs.size() + sizeof(long long) * b->psi0_off.size());
+    in += static_cast<int64_t>(sizeof(int) * b->obs.size());
+    for (const Bucket& bk : b->buckets) in += static_cast<int64_t>(sizeof(int) * bk.work.size());
+    if (h2d) *h2d = in;
+    if (d2h) *d2h = static_cast<int64_t>(sizeof(double) * b->rows_len + sizeof(int));
+  });
+}
+
+}  // extern "C"

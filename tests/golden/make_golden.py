@@ -79,6 +79,20 @@ def main() -> None:
             out[f"setup_{name}_{idx}_ref0_sha"] = np.frombuffer(bytes.fromhex(digest(s["ref0"])), dtype=np.uint8)
             out[f"setup_{name}_{idx}_psi0_head"] = s["psi0"][:32]
 
+    # The reference tests' own random states (DenseReference.cpp:204-214).
+    for L, seed in [(L, 0x9001 + L) for L in range(1, 7)] + [(4, 0x5150), (4, 0x2718), (5, 0x3141),
+                                                               (4, 0x1618), (3, 0x606), (3, 0x4004),
+                                                               (4, 0x1111), (4, 0x2222), (4, 0x4444)]:
+        out[f"ref_state_{L}_{seed}"] = ref.random_state(L, seed)
+    # Conservation over 10^4 steps of 0.02 at L=5 (test_Propagator.cpp:100-124),
+    # replayed on the reference's own state: final state, norm and energy drift.
+    from oracle.oracle import dense_hamiltonian
+    f, p, J = sample_hamiltonian(5)
+    psi = out["ref_state_5_12609"].copy()
+    for _ in range(100):
+        psi, _ = ref.evolve(5, f, p, J, psi, 0, 0.02, 100, eps=1e-12)
+    out["conservation_final"] = psi
+
     # Propagator steps on the reference's own sampleHamiltonian recipe.
     for L in range(1, 7):
         f, p, J = sample_hamiltonian(L)
