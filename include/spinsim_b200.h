@@ -191,6 +191,10 @@ int ss_axpy_sigma(double c, const ss_state* in, int spin, int axis,
 int ss_apply_sigma(const ss_state* in, int spin, int axis, ss_state* out);
 int ss_axpy_coupling(double jx, double jy, double jz, const ss_state* in,
                      int spin_a, int spin_b, ss_state* out);
+/* out += c * diag[k] * in[k] with a host diagonal of 2^L doubles
+   (SpinOperators.cpp:211-226 axpyDiagonal). */
+int ss_axpy_diagonal(double c, const double* diagonal, const ss_state* in,
+                     ss_state* out);
 /* out = sum_s sigma_axis(s) in  (src/ensemble/Ensemble.cpp:47-58,
    src/core/Observable.cpp:13-22) */
 int ss_apply_total_spin(int axis, const ss_state* in, ss_state* out);

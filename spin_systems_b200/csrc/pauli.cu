@@ -73,6 +73,19 @@ __global__ void k_total_spin(const double2* __restrict__ in, int nspins, int axi
   out[k] = make_double2(re, im);
 }
 
+// out += c * d[k] * in[k]  (SpinOperators.cpp:211-226)
+__global__ void k_axpy_diagonal(double c, const double* __restrict__ d,
+                                const double2* __restrict__ in, double2* out, size_t n) {
+  const size_t k = blockIdx.x * size_t{blockDim.x} + threadIdx.x;
+  if (k >= n) return;
+  const double f = c * d[k];
+  const double2 a = in[k];
+  double2 o = out[k];
+  o.x += f * a.x;
+  o.y += f * a.y;
+  out[k] = o;
+}
+
 inline unsigned int blocks_for(size_t n) {
   return static_cast<unsigned int>((n + kThreads - 1) / kThreads);
 }
@@ -134,6 +147,21 @@ int ss_axpy_coupling(double jx, double jy, double jz, const ss_state* in, int a,
     launch(in->engine, k_axpy_coupling, blocks_for(in->size()), kThreads, 0, jx - jy, jx + jy, jz,
            in->data, size_t{1} << (a < b ? a : b), size_t{1} << (a < b ? b : a), out->data,
            in->size());
+  });
+}
+
+int ss_axpy_diagonal(double c, const double* diagonal, const ss_state* in, ss_state* out) {
+  return guarded([&] {
+    check_distinct(in, out);
+    require(diagonal != nullptr, SS_ERR_INVALID_ARGUMENT, "null diagonal");
+    ss_engine* e = in->engine;
+    double* d = nullptr;
+    SS_CUDA(cudaMallocAsync(&d, sizeof(double) * in->size(), e->stream));
+    SS_CUDA(cudaMemcpyAsync(d, diagonal, sizeof(double) * in->size(), cudaMemcpyHostToDevice,
+                            e->stream));
+    launch(e, k_axpy_diagonal, blocks_for(in->size()), kThreads, 0, c, d, in->data, out->data,
+           in->size());
+    SS_CUDA(cudaFreeAsync(d, e->stream));
   });
 }
 

@@ -120,7 +120,27 @@ def main() -> None:
     t, v, _ = ref.run_range(cfg, 0, 2, 2)
     out["curves_xy8_l12_times"], out["curves_xy8_l12_rows"] = t, v
 
+    # Whole experiments (runExperiment with LocalRunner): mean/sd/stderr per
+    # (point, column) for the CLI's CSV, on this repository's L=10 CPMG config
+    # and on the reference's own example configs with few realisations.
+    from spin_systems_b200 import config as tomlcfg
+    for name, path, count in (("cpmg_l10", ROOT / "configs" / "cpmg_ideal_l10.toml", None),
+                              ("ref_cpmg8z", REFERENCE_TREE / "configs" / "cpmg8z.toml", 3),
+                              ("ref_rabi", REFERENCE_TREE / "configs" / "rabi_szsz.toml", 3)):
+        spec = tomlcfg.load(path, realizations=count)
+        t, m, sd, se, _ = ref.run_experiment(spec.config(), 4)
+        out[f"exp_{name}_times"], out[f"exp_{name}_mean"] = t, m
+        out[f"exp_{name}_sd"], out[f"exp_{name}_se"] = sd, se
+
     np.savez_compressed(OUT / "reference_outputs.npz", **out)
+    # The reference's example configurations as parsed documents (JSON), so the
+    # device runs can be checked against exp_ref_* where the reference tree
+    # is absent.
+    import json
+    import tomllib
+    docs = {name: tomllib.loads((REFERENCE_TREE / "configs" / f"{fname}.toml").read_text())
+            for name, fname in (("ref_cpmg8z", "cpmg8z"), ("ref_rabi", "rabi_szsz"))}
+    (OUT / "reference_configs.json").write_text(json.dumps(docs, indent=1, sort_keys=True))
     print("wrote", sorted(p.name for p in OUT.glob("*.npz")))
 
 

@@ -1,0 +1,188 @@
+"""The `spinsim` command line and its TOML reader against the reference's
+behaviour (apps/spinsim/main.cpp, src/io/Config.cpp, tests/test_Config.cpp).
+
+CPU: parsing, validation and error messages (no device needed).
+GPU: `spinsim run` CSV output against the reference's runExperiment."""
+import csv
+import io
+import json
+import math
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from spin_systems_b200 import config as tomlcfg
+
+ROOT = Path(__file__).resolve().parents[1]
+CLI = ROOT / "spin_systems_b200" / "bin" / "spinsim"
+CONFIGS = sorted((ROOT / "configs").glob("*.toml"))
+REFERENCE_CONFIGS = Path("/root/reference/configs")
+
+MINIMAL = """
+[system]
+spins = 3
+
+[field]
+hz = 1.0
+
+[measurement]
+observables = ["corr:z"]
+
+[[step]]
+kind = "measure"
+
+[[step]]
+kind = "evolve"
+tau = 0.1
+
+[[step]]
+kind = "measure"
+"""
+
+
+def cli(*args, check=False):
+    if not CLI.exists():
+        pytest.fail("spinsim binary missing: run __graft_entry__.build()")
+    r = subprocess.run([str(CLI), *map(str, args)], capture_output=True, text=True, timeout=600)
+    if check and r.returncode != 0:
+        raise AssertionError(r.stderr)
+    return r
+
+
+def write(tmp_path, text, name="c.toml"):
+    p = tmp_path / name
+    p.write_text(text)
+    return p
+
+
+def test_usage_and_exit_codes():
+    r = cli()
+    assert r.returncode == 2 and "Usage" in r.stdout
+    assert cli("--help").returncode == 0
+
+
+@pytest.mark.parametrize("path", CONFIGS, ids=[p.name for p in CONFIGS])
+def test_configs_validate_and_describe(path):
+    assert cli("validate", path).stdout.strip().endswith(": ok")
+    d = cli("describe", path, check=True).stdout
+    spec = tomlcfg.load(path)
+    assert f"spins           {spec.nspins}" in d
+    assert f"measurements    {spec.measurement_count()} per realization" in d
+
+
+@pytest.mark.skipif(not REFERENCE_CONFIGS.is_dir(), reason="reference tree not present")
+def test_reference_configs_parse():
+    for p in sorted(REFERENCE_CONFIGS.glob("*.toml")):
+        assert cli("validate", p).returncode == 0, p
+
+
+def test_minimal_config_and_overrides(tmp_path):
+    # test_Config.cpp:39-47, 116-138
+    d = cli("describe", write(tmp_path, MINIMAL), check=True).stdout
+    assert "measurements    2 per realization" in d
+    text = MINIMAL + '\n[[step]]\nkind = "repeat"\ncount = 3\nbody = [ { kind = "repeat", count = 4, body = [ { kind = "measure" } ] } ]\n'
+    d = cli("describe", write(tmp_path, text), check=True).stdout
+    assert "measurements    14 per realization" in d
+
+
+@pytest.mark.parametrize("text,needle", [
+    ('[system]\nspins = 3\n[field]\nhx = [1.0, 2.0]\n[measurement]\nobservables = ["norm"]\n[[step]]\nkind = "measure"\n', "hx"),
+    ('[system]\nspins = 2\n[measurement]\nobservables = ["norm"]\n[[step]]\nkind = "evolve"\ntau = 0.1\n', "'step'"),
+    ('[system]\nspins = 2\n[measurement]\nobservables = ["corr:w"]\n[[step]]\nkind = "measure"\n', "observables"),
+    ('[system]\nspins = 2\n[measurement]\nobservables = ["norm"]\n[[step]]\nkind = "teleport"\n', "teleport"),
+    ('[system\nspins = 2', "<syntax>"),
+    ('[system]\nspins = 99\n[measurement]\nobservables = ["norm"]\n[[step]]\nkind = "measure"\n', "system.spins"),
+    ('[system]\nspins = 2\n[measurement]\nobservables = ["norm"]\n[[step]]\nkind = "evolve"\ntau = 0.1\nsteps = -1\n[[step]]\nkind = "measure"\n', "steps"),
+    ('[system]\nspins = 2\n[measurement]\nobservables = ["norm"]\n[[step]]\nkind = "pulse"\nrotation = "pi:x:9"\n[[step]]\nkind = "measure"\n', "rotation"),
+    ('[system]\nspins = 2\n[measurement]\nobservables = ["norm"]\n[[step]]\nkind = "repeat"\ncount = 2\n', "body"),
+    ('[system]\nspins = 2\n[system]\nspins = 3\n', "<syntax>"),
+])
+def test_configuration_errors_name_the_key(tmp_path, text, needle):
+    r = cli("validate", write(tmp_path, text))
+    assert r.returncode == 1
+    assert needle in r.stderr and "c.toml" in r.stderr, r.stderr
+    if needle == "teleport":
+        assert "evolve" in r.stderr
+
+
+def test_unknown_option_and_bad_values(tmp_path):
+    p = write(tmp_path, MINIMAL)
+    assert cli("run", p, "--bogus").returncode == 1
+    assert cli("run", p, "--threads", "x").returncode == 1
+    assert cli("run", p, "--precision", "fp16").returncode == 1
+
+
+def read_csv(text):
+    rows = list(csv.reader(io.StringIO(text)))
+    header, body = rows[0], np.array([[float(x) for x in r] for r in rows[1:]])
+    return header, body
+
+
+def check_against(header, body, golden, name, atol):
+    times = golden[f"exp_{name}_times"]
+    mean, sd, se = golden[f"exp_{name}_mean"], golden[f"exp_{name}_sd"], golden[f"exp_{name}_se"]
+    ncols = (len(header) - 1) // 3
+    assert np.allclose(body[:, 0], times, rtol=1e-9, atol=1e-12)
+    got = body[:, 1:].reshape(len(times), ncols, 3)
+    want = np.stack([mean, sd, se], axis=-1).reshape(len(times), ncols, 3)
+    err = np.abs(got - want) - 1e-11 * np.abs(want)  # 12 significant digits in the CSV
+    assert err.max() < atol, err.max()
+
+
+def dump_toml(doc):
+    """A TOML writer for the parsed reference documents (tables, one array of
+    step tables, inline tables in arrays)."""
+    def val(v):
+        if isinstance(v, bool):
+            return "true" if v else "false"
+        if isinstance(v, (int, float)):
+            return repr(v)
+        if isinstance(v, str):
+            return json.dumps(v)
+        if isinstance(v, list):
+            return "[" + ", ".join(val(x) for x in v) + "]"
+        if isinstance(v, dict):
+            return "{ " + ", ".join(f"{k} = {val(x)}" for k, x in v.items()) + " }"
+        raise TypeError(v)
+    out = []
+    for k, v in doc.items():
+        if k == "step":
+            continue
+        out.append(f"[{k}]")
+        out += [f"{kk} = {val(vv)}" for kk, vv in v.items()]
+    for st in doc["step"]:
+        out.append("[[step]]")
+        out += [f"{kk} = {val(vv)}" for kk, vv in st.items()]
+    return "\n".join(out) + "\n"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("engine", ["batch", "plain"])
+def test_run_matches_reference_experiment(golden, engine):
+    r = cli("run", ROOT / "configs" / "cpmg_ideal_l10.toml", "--engine", engine, check=True)
+    header, body = read_csv(r.stdout)
+    assert header[:4] == ["time", "corr_x_re_mean", "corr_x_re_sd", "corr_x_re_stderr"]
+    check_against(header, body, golden, "cpmg_l10", 1e-10)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["ref_cpmg8z", "ref_rabi"])
+def test_reference_example_configs_run(golden, tmp_path, name):
+    docs = json.loads((ROOT / "tests" / "golden" / "reference_configs.json").read_text())
+    p = write(tmp_path, dump_toml(docs[name]), f"{name}.toml")
+    r = cli("run", p, "--realizations", "3", check=True)
+    header, body = read_csv(r.stdout)
+    check_against(header, body, golden, name, 1e-9)
+
+
+@pytest.mark.gpu
+def test_run_mixed_precision_and_output_file(golden, tmp_path):
+    out = tmp_path / "o" / "r.csv"
+    r = cli("run", ROOT / "configs" / "cpmg_ideal_l10.toml", "--precision", "mixed", "--out", out,
+            check=True)
+    assert "realizations on batched mixed" in r.stderr
+    header, body = read_csv(out.read_text())
+    mean = golden["exp_cpmg_l10_mean"].reshape(len(body), -1)
+    assert np.abs(body[:, 1] - mean[:, 0]).max() < 1e-5
