@@ -258,6 +258,17 @@ int ss_measure_corr(const ss_state* psi, const ss_state* ref, int axis,
 int ss_measure_mag(const ss_state* psi, int spin, int axis, double* out);
 int ss_measure_energy(const ss_ham* ham, const ss_state* psi, double* out);
 
+/* No counterpart in the reference: ss_measure_corr over caller-owned device
+ * vectors (2*2^nspins doubles each, re/im interleaved, 16-byte aligned, on
+ * the current device), allocating nothing.  Its scratch is a fixed ~19 KB
+ * array in the library's device memory; nspins outside [1, 30] is rejected
+ * with SS_ERR_OUT_OF_RANGE.  `stream` is a cudaStream_t (NULL = the legacy
+ * default stream); the call waits for it.  The first call on each device
+ * looks the scratch up (make it before any stream capture).  Calls that
+ * overlap on one device race on the scratch: serialise them. */
+int ss_measure_corr_noalloc(const double* psi, const double* ref, int nspins,
+                            int axis, void* stream, double out[2]);
+
 /* ------------------------------------------------------------ ensemble
  * Host-side, bit-for-bit with the reference's (seed, index) streams:
  * src/ensemble/Rng.cpp:8-23, Ensemble.cpp:20-112, io/Experiment.cpp:10-35.

@@ -98,6 +98,8 @@ def load(path: Path = LIB_PATH) -> C.CDLL:
     lib.ss_batch_create.argtypes = [C.c_void_p, C.POINTER(SsRunConfig), C.c_uint64, C.c_int64,
                                     C.c_int, C.POINTER(C.c_void_p)]
     lib.ss_run_realization.argtypes = [C.c_void_p, C.POINTER(SsRunConfig), C.c_uint64, _dp, _dp]
+    lib.ss_measure_corr_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p,
+                                            _dp]
     _lib = lib
     return lib
 
@@ -374,6 +376,15 @@ def two_spin_gate(psi: StateVector, m, a: int, b: int) -> None:
 def measure_corr(psi: StateVector, ref: StateVector, axis: int):
     out = (C.c_double * 2)()
     check(psi.lib.ss_measure_corr(psi.handle, ref.handle, axis, out))
+    return out[0], out[1]
+
+
+def measure_corr_noalloc(psi_ptr: int, ref_ptr: int, nspins: int, axis: int,
+                         stream: Optional[int] = None):
+    """ss_measure_corr over caller-owned device vectors (device addresses of
+    2*2^nspins doubles each), with no allocation; waits for `stream`."""
+    out = np.zeros(2)
+    check(load().ss_measure_corr_noalloc(psi_ptr, ref_ptr, nspins, axis, stream, _d(out)))
     return out[0], out[1]
 
 
