@@ -135,6 +135,11 @@ typedef struct ss_run_config {
   double tau_range[2];       /* if hi > lo: tau ~ U[lo, hi)              */
   int32_t n_spin_choices;    /* if > 0: L drawn uniformly from the list  */
   int32_t spin_choices[8];
+  /* additive: in SS_PRECISION_MIXED, a realisation whose Chebyshev orders
+     per state vector exceed this runs in the FP64 kernel of the same batch
+     (FP32 coefficient rounding grows with the order count); 0 = 40000,
+     negative = never.  Sizes without an FP64 kernel stay mixed. */
+  int64_t mixed_order_limit;
 } ss_run_config;
 
 /* ---------------------------------------------------------------- handles */
@@ -312,6 +317,12 @@ int ss_batch_stats(const ss_batch* batch, int64_t* orders,
                    double* amplitude_orders, int64_t* launches);
 /* Bytes ss_batch_run moves host->device (inputs) and device->host (rows). */
 int ss_batch_io_bytes(const ss_batch* batch, int64_t* h2d, int64_t* d2h);
+/* Per realisation, in index order (count entries each): the precision it
+   runs in (ss_precision; in a mixed batch those past mixed_order_limit are
+   FP64) and the amplitudes x orders it applies per run (both vectors).
+   Either output may be NULL. */
+int ss_batch_precisions(const ss_batch* batch, int32_t* precision,
+                        double* amplitude_orders);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

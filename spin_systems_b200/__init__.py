@@ -479,3 +479,14 @@ class Batch:
         check(self.lib.ss_batch_io_bytes(self.handle, C.byref(h2d), C.byref(d2h)))
         return dict(orders=orders.value, amplitude_orders=amp.value, launches=launches.value,
                     h2d_bytes=h2d.value, d2h_bytes=d2h.value)
+
+    def precisions(self) -> np.ndarray:
+        """The precision (abi.FP64 / abi.MIXED) each realisation runs in."""
+        return self.work()[0]
+
+    def work(self):
+        """(precision, amplitude-orders per run) of each realisation."""
+        prec = np.zeros(max(self.count, 1), dtype=np.int32)
+        amp = np.zeros(max(self.count, 1))
+        check(self.lib.ss_batch_precisions(self.handle, _i(prec), _d(amp)))
+        return prec[: self.count], amp[: self.count]

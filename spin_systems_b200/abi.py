@@ -54,6 +54,7 @@ class SsRunConfig(C.Structure):
         ("step_fields", C.POINTER(C.c_double)), ("draw_seed", C.c_uint64),
         ("disorder_range", C.c_double * 2), ("tau_range", C.c_double * 2),
         ("n_spin_choices", C.c_int32), ("spin_choices", C.c_int32 * 8),
+        ("mixed_order_limit", C.c_int64),
     ]
 
 
@@ -150,6 +151,7 @@ class RunSpec:
     disorder_range: Sequence[float] = (0.0, 0.0)
     tau_range: Sequence[float] = (0.0, 0.0)
     spin_choices: Sequence[int] = ()
+    mixed_order_limit: int = 0
 
     def __post_init__(self) -> None:
         self._keep: list = []
@@ -245,6 +247,7 @@ class RunSpec:
         c.n_spin_choices = len(self.spin_choices)
         for i, v in enumerate(self.spin_choices):
             c.spin_choices[i] = v
+        c.mixed_order_limit = int(self.mixed_order_limit)
         self._keep = [bf, st, ob, tf]
         return c
 

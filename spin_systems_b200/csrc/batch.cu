@@ -12,6 +12,8 @@
 #include <thread>
 #include <tuple>
 
+#include <cooperative_groups.h>
+
 #include "batch_kernel.cuh"
 #include "hamiltonian.cuh"
 
@@ -24,6 +26,9 @@ namespace batch {
 namespace {
 
 constexpr int kPrepThreads = 256;
+constexpr int kClusterSize = 2;  // state and reference of one realisation
+// Time of an FP64 amplitude-order relative to a mixed one (B200, L = 12).
+constexpr double kFp64CostFactor = 1.45;
 
 // ---------------------------------------------------------------- device
 __device__ __forceinline__ double2 sigma_at(const double2* in, uint32_t k, int s, int axis) {
@@ -59,7 +64,7 @@ __global__ void k_batch_prepare(const RealDev* reals, const double2* psi0, const
 
 template <int L, int R, typename Real, int PSI>
 __device__ void evolve_op(const Args& args, const Smem<Real>& sm, const RealDev& rd, double2* st,
-                          const Op& op, const TypeDev& ty) {
+                          const Op& op, const TypeDev& ty, int vec) {
   using Gm = Geo<L, R>;
   using C2 = typename Cplx<Real>::T;
   constexpr int NT = Gm::NT, NA = Gm::NA, G = Gm::G, N = Gm::N;
@@ -125,8 +130,8 @@ __device__ void evolve_op(const Args& args, const Smem<Real>& sm, const RealDev&
   const double2* wts = args.wpool + ty.w_off;
   const double a0 = wts[0].x;
 
-  for (int v = 0; v < 2; ++v) {
-    double2* psig = st + v * N;
+  {
+    double2* psig = st + vec * N;
     double2 preg[PSI == PSI_REG ? NA : 1] = {};
     // psi of amplitude slot a, wherever it lives
     auto psi_ld = [&](int a) -> double2 {
@@ -245,14 +250,14 @@ __device__ void evolve_op(const Args& args, const Smem<Real>& sm, const RealDev&
 }
 
 template <int NT>
-__device__ void pulse_op(const Args& args, int L, double2* st, const Op& op) {
+__device__ void pulse_op(const Args& args, int L, double2* st, const Op& op, int vec) {
   const double* u = args.rots + 8 * op.a;
   const double llr = u[0], lli = u[1], lhr = u[2], lhi = u[3];
   const double hlr = u[4], hli = u[5], hhr = u[6], hhi = u[7];
   const uint32_t n = 1u << L;
   const int s0 = op.b < 0 ? 0 : op.b, s1 = op.b < 0 ? L : op.b + 1;
-  for (int v = 0; v < 2; ++v) {
-    double2* psi = st + v * n;
+  {
+    double2* psi = st + vec * n;
     for (int s = s0; s < s1; ++s) {
       const uint32_t low = (1u << s) - 1u;
       for (uint32_t j = threadIdx.x; j < n / 2; j += NT) {
@@ -374,8 +379,14 @@ struct SmemLayout {
   static constexpr size_t total = at_red + 32 * sizeof(double2);
 };
 
+// One realisation per cluster of two CTAs: rank 0 carries the state, rank 1
+// the reference, each through every evolve and pulse of the program.  The
+// two meet only at measurements, where rank 0 reads both vectors from
+// global memory between two cluster barriers.  Co-scheduling of a cluster's
+// CTAs is guaranteed by the hardware, so the barriers always complete.
 template <int L, int R, typename Real, int PSI>
-__global__ void __launch_bounds__(Geo<L, R>::NT) k_batch(const __grid_constant__ Args args) {
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(Geo<L, R>::NT)
+    k_batch(const __grid_constant__ Args args) {
   using Gm = Geo<L, R>;
   using C2 = typename Cplx<Real>::T;
   using SL = SmemLayout<L, R, Real, PSI>;
@@ -397,12 +408,16 @@ __global__ void __launch_bounds__(Geo<L, R>::NT) k_batch(const __grid_constant__
   sm.corr_n = reinterpret_cast<int*>(smem_raw + SL::at_corr + kCorr * (sizeof(double2) + sizeof(uint2)));
   sm.red = reinterpret_cast<double2*>(smem_raw + SL::at_red);
   __shared__ int s_work;
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  const int vec = static_cast<int>(cluster.block_rank());
+  int* lead_work = cluster.map_shared_rank(&s_work, 0);
 
   for (;;) {
-    if (threadIdx.x == 0) s_work = static_cast<int>(atomicAdd(args.counter, 1u));
-    __syncthreads();
-    const int w = s_work;
-    __syncthreads();
+    if (vec == 0 && threadIdx.x == 0) s_work = static_cast<int>(atomicAdd(args.counter, 1u));
+    cluster.sync();
+    const int w = *lead_work;
+    cluster.sync();  // rank 1 has read the item before rank 0 may fetch again
     if (w >= args.nwork) break;
     const RealDev rd = args.reals[args.work[w]];
     double2* st = args.states + rd.state_off;
@@ -410,11 +425,16 @@ __global__ void __launch_bounds__(Geo<L, R>::NT) k_batch(const __grid_constant__
       const Op op = args.ops[i];
       if (op.kind == OP_EVOLVE) {
         const TypeDev ty = args.types[rd.type_off + op.a];
-        if (ty.order > 0 && op.b > 0) evolve_op<L, R, Real, PSI>(args, sm, rd, st, op, ty);
+        if (ty.order > 0 && op.b > 0) evolve_op<L, R, Real, PSI>(args, sm, rd, st, op, ty, vec);
       } else if (op.kind == OP_PULSE) {
-        pulse_op<NT>(args, L, st, op);
+        pulse_op<NT>(args, L, st, op, vec);
       } else {
-        measure_op<L, NT>(args, reinterpret_cast<double2*>(smem_raw), sm.red, rd, st, op);
+        __threadfence();
+        cluster.sync();  // both vectors are at this point of the program
+        if (vec == 0) {
+          measure_op<L, NT>(args, reinterpret_cast<double2*>(smem_raw), sm.red, rd, st, op);
+        }
+        cluster.sync();  // the reference stays put until it has been read
       }
     }
   }
@@ -514,6 +534,8 @@ struct ss_batch {
   int64_t orders_total = 0;
   double amp_orders = 0.0;
   int64_t launches_per_run = 0;
+  std::vector<int32_t> real_precision;  // ss_precision per realisation, index order
+  std::vector<double> real_amp_orders;  // amplitudes x orders per realisation
   // device
   Op* d_ops = nullptr;
   double* d_rots = nullptr;
@@ -647,6 +669,7 @@ struct PerReal {
   double cost = 0.0;
   int64_t orders = 0;
   double amp_orders = 0.0;
+  bool mixed = false;
   int error = 0;
   std::string message;
 };
@@ -684,6 +707,18 @@ void exact_transverse(int L, const double* f, int mode, double tau, Expansion& e
   ex.bound = bound2;
 }
 
+constexpr int64_t kDefaultMixedOrderLimit = 40000;
+
+// Mixed precision stores every coefficient as one FP32 number; the rounding
+// is a fixed perturbation of the Hamiltonian whose effect on the echo grows
+// with the number of orders applied.  A realisation past `limit` orders per
+// state vector therefore runs in FP64 (when its size has an FP64 kernel).
+bool stays_mixed(const ss_run_config& c, int L, int64_t orders_per_state) {
+  const int64_t limit = c.mixed_order_limit == 0 ? kDefaultMixedOrderLimit : c.mixed_order_limit;
+  if (limit < 0 || orders_per_state <= limit) return true;
+  return find_variant(L, false) == nullptr;
+}
+
 void build_realization(const ss_run_config& c, uint64_t index, const std::vector<TypeKey>& keys,
                        const std::vector<Op>& ops, bool mixed, PerReal& out) {
   try {
@@ -694,13 +729,28 @@ void build_realization(const ss_run_config& c, uint64_t index, const std::vector
     for (const PairTerm& p : rz.pairs) out.pairs.push_back(make_int2(p.lo, p.hi));
     const int L = rz.nspins;
     std::vector<int> orders(keys.size(), 0);
+    std::vector<Expansion> exps;
+    std::vector<const double*> tables;
     for (size_t t = 0; t < keys.size(); ++t) {
       const TypeKey& k = keys[t];
       const double* f = k.table >= 0 ? c.step_fields + static_cast<size_t>(3) * c.nspins * k.table
                                      : rz.fields.data();
       const double tau = k.from_draw ? k.tau * rz.tau_draw : k.tau;
-      Expansion ex = chebyshev(k.mode, spectral_bound(L, f, rz.pairs), tau, c.epsilon);
-      if (mixed) exact_transverse(L, f, k.mode, tau, ex);
+      exps.push_back(chebyshev(k.mode, spectral_bound(L, f, rz.pairs), tau, c.epsilon));
+      tables.push_back(f);
+      orders[t] = static_cast<int>(exps.back().order());
+    }
+    int64_t per_state = 0;
+    for (const Op& op : ops) {
+      if (op.kind == OP_EVOLVE) per_state += static_cast<int64_t>(orders[op.a]) * op.b;
+    }
+    out.mixed = mixed && stays_mixed(c, L, per_state);
+    for (size_t t = 0; t < keys.size(); ++t) {
+      const TypeKey& k = keys[t];
+      const double* f = tables[t];
+      const double tau = k.from_draw ? k.tau * rz.tau_draw : k.tau;
+      Expansion& ex = exps[t];
+      if (out.mixed) exact_transverse(L, f, k.mode, tau, ex);
       TypeDev ty{};
       ty.order = static_cast<int>(ex.order());
       orders[t] = ty.order;
@@ -780,7 +830,7 @@ void build_plan(ss_batch* b, const ss_run_config& c) {
   }
 
   long long state_off = 0, row_off = 0;
-  std::map<int, std::vector<int>> by_size;
+  std::map<std::pair<int, bool>, std::vector<int>> by_size;
   for (size_t i = 0; i < per.size(); ++i) {
     PerReal& pr = per[i];
     for (int o = 0; o < c.n_observables; ++o) {
@@ -813,7 +863,9 @@ void build_plan(ss_batch* b, const ss_run_config& c) {
     row_off += b->points * b->width;
     b->orders_total += pr.orders;
     b->amp_orders += pr.amp_orders;
-    by_size[pr.L].push_back(static_cast<int>(i));
+    by_size[{pr.L, pr.mixed}].push_back(static_cast<int>(i));
+    b->real_precision.push_back(pr.mixed ? SS_PRECISION_MIXED : SS_PRECISION_FP64);
+    b->real_amp_orders.push_back(pr.amp_orders);
   }
   b->state_len = state_off;
   b->rows_len = row_off;
@@ -833,9 +885,14 @@ void build_plan(ss_batch* b, const ss_run_config& c) {
     }
   }
 
-  const bool mixed = b->precision == SS_PRECISION_MIXED;
-  ss_engine* e = b->engine;
-  for (auto& [L, list] : by_size) {
+  // Buckets (one per size and precision) run side by side.  Each gets a
+  // share of the device in proportion to its cost, in clusters that can be
+  // resident together, so that no bucket's persistent CTAs wait for another
+  // bucket to drain; within a bucket the most expensive realisations go first.
+  std::vector<double> weight;
+  double total_weight = 0.0;
+  for (auto& [key, list] : by_size) {
+    const auto [L, mixed] = key;
     Bucket bk;
     bk.L = L;
     bk.var = find_variant(L, mixed);
@@ -847,14 +904,28 @@ void build_plan(ss_batch* b, const ss_run_config& c) {
     std::stable_sort(list.begin(), list.end(),
                      [&](int x, int y) { return per[x].cost > per[y].cost; });
     bk.work = list;
+    double w = 0.0;
+    for (int x : list) w += per[x].cost;
+    w *= mixed ? 1.0 : kFp64CostFactor;
+    weight.push_back(w);
+    total_weight += w;
+    b->buckets.push_back(std::move(bk));
+  }
+  for (size_t i = 0; i < b->buckets.size(); ++i) {
+    Bucket& bk = b->buckets[i];
     SS_CUDA(cudaFuncSetAttribute(bk.var->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(bk.var->smem)));
-    int per_sm = 0;
-    SS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bk.var->kernel,
-                                                          bk.var->threads, bk.var->smem));
-    require(per_sm > 0, SS_ERR_RUNTIME, "batched kernel does not fit an SM");
-    bk.grid = std::min<int>(per_sm * e->sm_count, static_cast<int>(list.size()));
-    b->buckets.push_back(std::move(bk));
+    cudaLaunchConfig_t lc{};
+    lc.gridDim = dim3(2 * kClusterSize);
+    lc.blockDim = dim3(bk.var->threads);
+    lc.dynamicSmemBytes = bk.var->smem;
+    int resident = 0;
+    SS_CUDA(cudaOccupancyMaxActiveClusters(&resident, bk.var->kernel, &lc));
+    require(resident > 0, SS_ERR_RUNTIME, "batched kernel cluster does not fit the device");
+    const double share = total_weight > 0.0 ? weight[i] / total_weight : 1.0;
+    int clusters = static_cast<int>(share * resident);
+    clusters = std::max(1, std::min<int>(clusters, static_cast<int>(bk.work.size())));
+    bk.grid = kClusterSize * clusters;
   }
 }
 
@@ -1108,6 +1179,16 @@ int ss_batch_io_bytes(const ss_batch* b, int64_t* h2d, int64_t* d2h) {
     for (const Bucket& bk : b->buckets) in += static_cast<int64_t>(sizeof(int) * bk.work.size());
     if (h2d) *h2d = in;
     if (d2h) *d2h = static_cast<int64_t>(sizeof(double) * b->rows_len + sizeof(int));
+  });
+}
+
+int ss_batch_precisions(const ss_batch* b, int32_t* precision, double* amplitude_orders) {
+  return guarded([&] {
+    require(b != nullptr, SS_ERR_INVALID_ARGUMENT, "null batch");
+    if (precision) std::copy(b->real_precision.begin(), b->real_precision.end(), precision);
+    if (amplitude_orders) {
+      std::copy(b->real_amp_orders.begin(), b->real_amp_orders.end(), amplitude_orders);
+    }
   });
 }
 

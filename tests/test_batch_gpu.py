@@ -98,6 +98,59 @@ def test_mixed_against_fp64_batch_many_realisations(engine):
     assert err.max() < ECHO_TOL, err.max()
 
 
+def orders_per_state(port, spec, count):
+    """Chebyshev orders per state vector of each XY-8 realisation."""
+    cfg, L = spec.config(), spec.nspins
+    fx = np.array(spec.fields_for(hx=50.0)).ravel()
+    fy = np.array(spec.fields_for(hy=50.0)).ravel()
+    blocks = spec.steps[0].count
+    out = []
+    for i in range(count):
+        s = port.setup(cfg, i, L)
+        total = 0
+        # per XY-8 block: 16 half-intervals, 4 x pulses, 4 y pulses
+        for f, tau, n in ((s["fields"], 0.125, 16 * blocks), (fx, np.pi / 50, 4 * blocks),
+                          (fy, np.pi / 50, 4 * blocks)):
+            a, _ = port.chebyshev(0, port.spectral_bound(L, f, s["J"]), tau, spec.epsilon)
+            total += (len(a) - 1) * n
+        out.append(total)
+    return np.array(out)
+
+
+def test_mixed_routes_long_realisations_to_fp64(engine, port):
+    # Full XY-8 x 16 at L = 12: realisations past 40000 orders per state run
+    # in the FP64 kernel of the same batch, bit-identical to an FP64 batch.
+    n = 192
+    spec = workloads.xy8_finite(realizations=n)
+    orders = orders_per_state(port, spec, n)
+    b = ss.Batch(engine, spec.config(), 0, n, abi.MIXED)
+    prec = b.precisions()
+    assert np.array_equal(prec == abi.FP64, orders > 40000)
+    assert (prec == abi.FP64).any() and (prec == abi.MIXED).any()
+    _, mixed = b.run()
+    _, fp64 = run(engine, spec, n, abi.FP64)
+    routed = prec == abi.FP64
+    assert np.array_equal(mixed[routed], fp64[routed])
+    err = echo_error(mixed, fp64, corr0(spec, n))
+    assert err.max() < ECHO_TOL, (err.max(), int(err.argmax()))
+
+
+def test_mixed_order_limit_switches(engine):
+    spec = workloads.xy8_finite(nspins=10, realizations=6, blocks=2)
+    spec.mixed_order_limit = 1
+    b = ss.Batch(engine, spec.config(), 0, 6, abi.MIXED)
+    assert (b.precisions() == abi.FP64).all()
+    _, every = b.run()
+    _, fp64 = run(engine, spec, 6, abi.FP64)
+    assert np.array_equal(every, fp64)
+    spec.mixed_order_limit = -1
+    assert (ss.Batch(engine, spec.config(), 0, 6, abi.MIXED).precisions() == abi.MIXED).all()
+    spec13 = workloads.xy8_finite(nspins=13, realizations=2, blocks=1)
+    spec13.mixed_order_limit = 1  # no FP64 kernel at L = 13: stays mixed
+    assert (ss.Batch(engine, spec13.config(), 0, 2, abi.MIXED).precisions() == abi.MIXED).all()
+    assert (ss.Batch(engine, spec.config(), 0, 6, abi.FP64).precisions() == abi.FP64).all()
+
+
 def test_uneven_sizes_share_one_launch(engine, port):
     spec = workloads.cpmg_uneven(realizations=12, pulses=4)
     spec.spin_choices = (8, 10, 12)
