@@ -36,6 +36,9 @@ L = 12
 MIXED_BYTES_PER_AMP_ORDER = 56.0   # FP32 T_{n-1}, T_{n-2}, T_n + FP64 psi read+write
 FP64_BYTES_PER_AMP_ORDER = 80.0    # FP64 T_{n-1}, T_{n-2}, T_n + FP64 psi read+write
 SMEM_BYTES_PER_AMP_ORDER = 168.0   # shared-memory traffic of the L=12, R=4 FP32 schedule
+# DRAM bytes per amplitude-order of k_batch<12,4,float>: ncu capture of
+# profile_case (296 realisations, 2 XY-8 blocks): 48.2 MB for 6.149e9.
+DRAM_BYTES_PER_AMP_ORDER_MEASURED = 48.215296e6 / 6.149e9
 FLOPS_PER_AMP_ORDER = L * (L - 1) * 2 + 20
 
 
@@ -287,7 +290,11 @@ def run_ours(args):
                 "h2d_bytes_per_step": stats["h2d_bytes"], "d2h_bytes_per_step": stats["d2h_bytes"]},
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": None, "peak_source": src,
+                     "frac": achieved / hbm,
+                     "traffic": DRAM_BYTES_PER_AMP_ORDER_MEASURED * amp_mixed,
+                     "traffic_note": "DRAM bytes of the mixed kernel per launch, scaled from "
+                                     "an ncu capture of a smaller case by amplitude-orders",
+                     "peak_source": src,
                      "kernel": "k_batch<12,4,float> with the routed realisations in "
                                "k_batch<12,3,double> of the same graph (state vectors resident "
                                "in shared memory)",
