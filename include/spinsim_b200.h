@@ -140,6 +140,16 @@ typedef struct ss_run_config {
      (FP32 coefficient rounding grows with the order count); 0 = 40000,
      negative = never.  Sizes without an FP64 kernel stay mixed. */
   int64_t mixed_order_limit;
+  /* additive: a parameter sweep for the batched engine.  With
+     sweep_points = P > 0 a batch of `count` realisations is P consecutive
+     blocks of count / P; slot s of point p = s / (count / P) draws its
+     geometry, fields and initial state for index first + s % (count / P)
+     (every point sees the same realisations) and takes the point's row of
+     sweep_params = (dipolar_scale, field_disorder, tau for tau_from_draw
+     steps, pulse-angle scale). */
+  int32_t sweep_points;
+  int32_t reserved1;
+  const double* sweep_params; /* 4 * sweep_points */
 } ss_run_config;
 
 /* ---------------------------------------------------------------- handles */
@@ -323,6 +333,43 @@ int ss_batch_io_bytes(const ss_batch* batch, int64_t* h2d, int64_t* d2h);
    Either output may be NULL. */
 int ss_batch_precisions(const ss_batch* batch, int32_t* precision,
                         double* amplitude_orders);
+
+/* -------------------------------------------------------- echo surrogate
+ * No counterpart in the reference (its parameter sweeps always run the
+ * exact propagator, io/Experiment.cpp:57-72).  A 6 -> 256 -> 256 -> 256 ->
+ * 128 GELU MLP mapping (areal density, field sigma, tau, pulse-angle error,
+ * sequence, L), each normalised by the caller, to the disorder-averaged
+ * S^x echo at 128 times.  BF16 weights and activations, FP32 accumulation,
+ * FP32 master weights under Adam; every product runs on the tcgen05 tensor
+ * cores.  Parameters are flat FP32 in the order W0[256][6] b0[256]
+ * W1[256][256] b1 W2[256][256] b2 W3[128][256] b3[128] (ss_mlp_param_count
+ * values).  `batch` rows go through the device per pass (a multiple of
+ * 128); inputs are rows of 6 floats, outputs and targets rows of 128. */
+typedef struct ss_mlp ss_mlp;
+int64_t ss_mlp_param_count(void);
+int ss_mlp_create(ss_engine* engine, int batch, uint64_t seed, ss_mlp** out);
+int ss_mlp_destroy(ss_mlp* net);
+int ss_mlp_get_params(const ss_mlp* net, float* params);
+/* Replaces every parameter and resets the Adam state. */
+int ss_mlp_set_params(ss_mlp* net, const float* params);
+/* y[rows][128] = net(x[rows][6]); any number of rows. */
+int ss_mlp_forward(ss_mlp* net, const float* x, int64_t rows, float* y);
+/* Gradient of the mean-squared error over rows (1..batch) of x and target
+ * with respect to every parameter (flat order), and the loss; no update. */
+int ss_mlp_gradients(ss_mlp* net, const float* x, const float* target,
+                     int64_t rows, float* grads, double* loss);
+/* Uploads a training set (rows >= batch) that stays on the device. */
+int ss_mlp_set_data(ss_mlp* net, const float* x, const float* y, int64_t rows);
+/* `steps` Adam steps (beta 0.9 / 0.999) on shuffled batches of the training
+ * set, learning rate on a cosine from lr_start to lr_end; losses (steps
+ * values, may be NULL) receives each step's batch loss. */
+int ss_mlp_train(ss_mlp* net, int64_t steps, float lr_start, float lr_end,
+                 uint64_t seed, double* losses);
+/* The surrogate's tensor-core product on its own, for verification:
+ * c[M][N] = a[M][K] b[N][K]^T with a and b raw BF16 bit patterns, FP32
+ * accumulation; M % 128 == 0, K % 64 == 0, N % 16 == 0 and N <= 256. */
+int ss_mlp_gemm_test(ss_engine* engine, const uint16_t* a, const uint16_t* b,
+                     int M, int N, int K, float* c);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

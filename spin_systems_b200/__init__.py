@@ -490,3 +490,95 @@ class Batch:
         amp = np.zeros(max(self.count, 1))
         check(self.lib.ss_batch_precisions(self.handle, _i(prec), _d(amp)))
         return prec[: self.count], amp[: self.count]
+
+
+# ------------------------------------------------------------ echo surrogate
+_fp = C.POINTER(C.c_float)
+
+
+def _f(a: np.ndarray):
+    return a.ctypes.data_as(_fp)
+
+
+class Mlp:
+    """The surrogate network on the device (ss_mlp_*): 6 -> 256 -> 256 ->
+    256 -> 128 GELU MLP, BF16 weights/activations, FP32 accumulation, trained
+    with Adam by the library's own tensor-core kernels."""
+
+    def __init__(self, engine: Engine, batch: int = 1024, seed: int = 0):
+        self.engine, self.lib = engine, engine.lib
+        self.lib.ss_mlp_param_count.restype = C.c_int64
+        self.lib.ss_mlp_create.argtypes = [C.c_void_p, C.c_int, C.c_uint64, C.POINTER(C.c_void_p)]
+        self.lib.ss_mlp_forward.argtypes = [C.c_void_p, _fp, C.c_int64, _fp]
+        self.lib.ss_mlp_gradients.argtypes = [C.c_void_p, _fp, _fp, C.c_int64, _fp,
+                                              C.POINTER(C.c_double)]
+        self.lib.ss_mlp_set_data.argtypes = [C.c_void_p, _fp, _fp, C.c_int64]
+        self.lib.ss_mlp_train.argtypes = [C.c_void_p, C.c_int64, C.c_float, C.c_float, C.c_uint64,
+                                          _dp]
+        self.lib.ss_mlp_get_params.argtypes = [C.c_void_p, _fp]
+        self.lib.ss_mlp_set_params.argtypes = [C.c_void_p, _fp]
+        h = C.c_void_p()
+        check(self.lib.ss_mlp_create(engine.handle, batch, seed, C.byref(h)))
+        self.handle, self.batch = h, batch
+        self.nparams = int(self.lib.ss_mlp_param_count())
+        engine._adopt(self)
+
+    def _destroy(self) -> None:
+        if getattr(self, "handle", None):
+            self.lib.ss_mlp_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self._destroy()
+        except Exception:
+            pass
+
+    def params(self) -> np.ndarray:
+        p = np.zeros(self.nparams, dtype=np.float32)
+        check(self.lib.ss_mlp_get_params(self.handle, _f(p)))
+        return p
+
+    def set_params(self, p) -> None:
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        assert p.size == self.nparams
+        check(self.lib.ss_mlp_set_params(self.handle, _f(p)))
+
+    def forward(self, x) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, 6)
+        y = np.zeros((max(len(x), 1), 128), dtype=np.float32)
+        check(self.lib.ss_mlp_forward(self.handle, _f(x), len(x), _f(y)))
+        return y[: len(x)]
+
+    def gradients(self, x, target):
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, 6)
+        t = np.ascontiguousarray(target, dtype=np.float32).reshape(-1, 128)
+        g = np.zeros(self.nparams, dtype=np.float32)
+        loss = C.c_double()
+        check(self.lib.ss_mlp_gradients(self.handle, _f(x), _f(t), len(x), _f(g), C.byref(loss)))
+        return loss.value, g
+
+    def set_data(self, x, y) -> None:
+        self._x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, 6)
+        self._y = np.ascontiguousarray(y, dtype=np.float32).reshape(-1, 128)
+        check(self.lib.ss_mlp_set_data(self.handle, _f(self._x), _f(self._y), len(self._x)))
+
+    def train(self, steps: int, lr_start: float = 1e-3, lr_end: float = 1e-5,
+              seed: int = 0) -> np.ndarray:
+        losses = np.zeros(max(steps, 1))
+        check(self.lib.ss_mlp_train(self.handle, steps, lr_start, lr_end, seed, _d(losses)))
+        return losses[:steps]
+
+
+def mlp_gemm_test(engine: Engine, a_bits: np.ndarray, b_bits: np.ndarray) -> np.ndarray:
+    """c = a b^T on the surrogate's tensor-core GEMM (BF16 bit patterns in)."""
+    a = np.ascontiguousarray(a_bits, dtype=np.uint16)
+    b = np.ascontiguousarray(b_bits, dtype=np.uint16)
+    M, K = a.shape
+    N = b.shape[0]
+    c = np.zeros((M, N), dtype=np.float32)
+    u16 = C.POINTER(C.c_uint16)
+    engine.lib.ss_mlp_gemm_test.argtypes = [C.c_void_p, u16, u16, C.c_int, C.c_int, C.c_int, _fp]
+    check(engine.lib.ss_mlp_gemm_test(engine.handle, a.ctypes.data_as(u16), b.ctypes.data_as(u16),
+                                      M, N, K, _f(c)))
+    return c

@@ -55,6 +55,8 @@ class SsRunConfig(C.Structure):
         ("disorder_range", C.c_double * 2), ("tau_range", C.c_double * 2),
         ("n_spin_choices", C.c_int32), ("spin_choices", C.c_int32 * 8),
         ("mixed_order_limit", C.c_int64),
+        ("sweep_points", C.c_int32), ("reserved1", C.c_int32),
+        ("sweep_params", C.POINTER(C.c_double)),
     ]
 
 

@@ -6,6 +6,7 @@
 // Chebyshev series weights, prescaled couplings).  Device side: see
 // batch_kernel.cuh.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <map>
 #include <numeric>
@@ -250,8 +251,9 @@ __device__ void evolve_op(const Args& args, const Smem<Real>& sm, const RealDev&
 }
 
 template <int NT>
-__device__ void pulse_op(const Args& args, int L, double2* st, const Op& op, int vec) {
-  const double* u = args.rots + 8 * op.a;
+__device__ void pulse_op(const Args& args, int L, double2* st, const Op& op, int vec,
+                         long long rot_off) {
+  const double* u = args.rots + rot_off + 8 * op.a;
   const double llr = u[0], lli = u[1], lhr = u[2], lhi = u[3];
   const double hlr = u[4], hli = u[5], hhr = u[6], hhi = u[7];
   const uint32_t n = 1u << L;
@@ -427,7 +429,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(Geo<L, R>::NT)
         const TypeDev ty = args.types[rd.type_off + op.a];
         if (ty.order > 0 && op.b > 0) evolve_op<L, R, Real, PSI>(args, sm, rd, st, op, ty, vec);
       } else if (op.kind == OP_PULSE) {
-        pulse_op<NT>(args, L, st, op, vec);
+        pulse_op<NT>(args, L, st, op, vec, rd.rot_off);
       } else {
         __threadfence();
         cluster.sync();  // both vectors are at this point of the program
@@ -574,7 +576,7 @@ void upload_vec(T* dst, const std::vector<T>& src, cudaStream_t s) {
 void linearise(const ss_run_config& c, int begin, int end, std::vector<Op>& ops,
                std::map<TypeKey, int>& types, std::vector<TypeKey>& keys,
                std::map<std::vector<double>, int>& rot_ids, std::vector<double>& rots,
-               int64_t& point) {
+               std::vector<std::array<double, 4>>& rot_src, int64_t& point) {
   for (int at = begin; at < end;) {
     const ss_step& s = c.steps[at];
     if (s.kind == SS_STEP_EVOLVE) {
@@ -595,6 +597,7 @@ void linearise(const ss_run_config& c, int begin, int end, std::vector<Op>& ops,
       if (it == rot_ids.end()) {
         it = rot_ids.emplace(key, static_cast<int>(rots.size() / 8)).first;
         rots.insert(rots.end(), u, u + 8);
+        rot_src.push_back({s.axis[0], s.axis[1], s.axis[2], s.angle});
       }
       ops.push_back(Op{OP_PULSE, it->second, s.target, 0});
       ++at;
@@ -603,7 +606,7 @@ void linearise(const ss_run_config& c, int begin, int end, std::vector<Op>& ops,
       ++at;
     } else {
       for (int64_t i = 0; i < s.count; ++i) {
-        linearise(c, at + 1, at + 1 + s.body_len, ops, types, keys, rot_ids, rots, point);
+        linearise(c, at + 1, at + 1 + s.body_len, ops, types, keys, rot_ids, rots, rot_src, point);
       }
       at += 1 + s.body_len;
     }
@@ -720,9 +723,11 @@ bool stays_mixed(const ss_run_config& c, int L, int64_t orders_per_state) {
 }
 
 void build_realization(const ss_run_config& c, uint64_t index, const std::vector<TypeKey>& keys,
-                       const std::vector<Op>& ops, bool mixed, PerReal& out) {
+                       const std::vector<Op>& ops, bool mixed, PerReal& out,
+                       double tau_override = 0.0) {
   try {
-    const Realization rz = assemble_realization(c, index);
+    Realization rz = assemble_realization(c, index);
+    if (tau_override > 0.0) rz.tau_draw = tau_override;
     out.L = rz.nspins;
     out.tau_draw = rz.tau_draw;
     out.psi0 = rz.psi0;
@@ -791,8 +796,31 @@ void build_plan(ss_batch* b, const ss_run_config& c) {
   std::map<TypeKey, int> type_ids;
   std::vector<TypeKey> keys;
   std::map<std::vector<double>, int> rot_ids;
+  std::vector<std::array<double, 4>> rot_src;
   int64_t point = 0;
-  linearise(c, 0, c.n_steps, b->ops, type_ids, keys, rot_ids, b->rots, point);
+  linearise(c, 0, c.n_steps, b->ops, type_ids, keys, rot_ids, b->rots, rot_src, point);
+  // A sweep: consecutive blocks of realisation slots share the geometry
+  // indices first .. first + per_point - 1 and take their point's scales;
+  // rotation table 1 + p holds the pulses of point p with scaled angles.
+  const int64_t npoints = c.sweep_points;
+  int64_t per_point = b->count;
+  if (npoints > 0) {
+    require(c.sweep_params != nullptr && b->count % npoints == 0, SS_ERR_INVALID_ARGUMENT,
+            "a sweep needs sweep_params and a realisation count divisible by sweep_points");
+    per_point = b->count / npoints;
+    const size_t nrot = rot_src.size();
+    for (int64_t q = 0; q < npoints; ++q) {
+      const double* sp = c.sweep_params + 4 * q;
+      require(sp[0] >= 0.0 && sp[1] >= 0.0 && sp[2] > 0.0 && std::isfinite(sp[3]),
+              SS_ERR_INVALID_ARGUMENT, "sweep parameters out of range");
+      for (size_t r = 0; r < nrot; ++r) {
+        double u[8];
+        const double axis[3] = {rot_src[r][0], rot_src[r][1], rot_src[r][2]};
+        rotation_matrix(axis, rot_src[r][3] * sp[3], u);
+        b->rots.insert(b->rots.end(), u, u + 8);
+      }
+    }
+  }
   b->points = point;
   b->width = observable_width(c.observables, c.n_observables);
   b->ntypes = static_cast<int>(keys.size());
@@ -818,8 +846,17 @@ void build_plan(ss_batch* b, const ss_run_config& c) {
     for (size_t w = 0; w < workers; ++w) {
       pool.emplace_back([&] {
         for (size_t i = next.fetch_add(1); i < per.size(); i = next.fetch_add(1)) {
-          build_realization(c, b->first + i, keys, b->ops, b->precision == SS_PRECISION_MIXED,
-                            per[i]);
+          if (npoints > 0) {
+            const double* sp = c.sweep_params + 4 * (static_cast<int64_t>(i) / per_point);
+            ss_run_config ci = c;
+            ci.dipolar_scale = sp[0];
+            ci.field_disorder = sp[1];
+            build_realization(ci, b->first + i % per_point, keys, b->ops,
+                              b->precision == SS_PRECISION_MIXED, per[i], sp[2]);
+          } else {
+            build_realization(c, b->first + i, keys, b->ops, b->precision == SS_PRECISION_MIXED,
+                              per[i]);
+          }
         }
       });
     }
@@ -846,6 +883,10 @@ void build_plan(ss_batch* b, const ss_run_config& c) {
     rd.state_off = state_off;
     rd.type_off = static_cast<long long>(b->types.size());
     rd.row_off = row_off;
+    rd.rot_off = npoints > 0
+                     ? static_cast<long long>(8 * rot_src.size()) *
+                           (1 + static_cast<long long>(i) / per_point)
+                     : 0;
     const long long c_base = static_cast<long long>(b->cpool.size());
     const long long w_base = static_cast<long long>(b->wpool.size() / 2);
     for (TypeDev ty : pr.types) {

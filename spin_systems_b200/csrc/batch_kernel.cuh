@@ -69,6 +69,7 @@ struct RealDev {
   long long state_off;  // 2 * 2^L double2: state, then reference
   long long type_off;   // first TypeDev of this realisation
   long long row_off;    // first value of its measurement rows
+  long long rot_off;    // its rotation table in the rotation pool (sweeps)
 };
 
 struct Args {
