@@ -154,6 +154,9 @@ class RunSpec:
     tau_range: Sequence[float] = (0.0, 0.0)
     spin_choices: Sequence[int] = ()
     mixed_order_limit: int = 0
+    # additive: a parameter sweep for the batched engine, one row per point
+    # (dipolar_scale, field_disorder, tau of tau_from_draw steps, angle scale)
+    sweep: Optional[Sequence[Sequence[float]]] = None
 
     def __post_init__(self) -> None:
         self._keep: list = []
@@ -250,7 +253,15 @@ class RunSpec:
         for i, v in enumerate(self.spin_choices):
             c.spin_choices[i] = v
         c.mixed_order_limit = int(self.mixed_order_limit)
-        self._keep = [bf, st, ob, tf]
+        sw = None
+        if self.sweep is not None and len(self.sweep) > 0:
+            flat_sw = [float(v) for row in self.sweep for v in row]
+            if len(flat_sw) != 4 * len(self.sweep):
+                raise ValueError("a sweep row is (dipolar_scale, field_disorder, tau, angle_scale)")
+            sw = (C.c_double * len(flat_sw))(*flat_sw)
+            c.sweep_points = len(self.sweep)
+            c.sweep_params = C.cast(sw, C.POINTER(C.c_double))
+        self._keep = [bf, st, ob, tf, sw]
         return c
 
     def max_spins(self) -> int:

@@ -442,6 +442,438 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(Geo<L, R>::NT)
   }
 }
 
+// ------------------------------------------------- vectors over a cluster
+// Sizes whose three recursion buffers exceed one CTA's shared memory spread
+// each vector over C = 2^CB CTAs of the cluster: CTA `part` of a vector holds
+// the amplitudes whose top CB bits equal `part`, with the same layout schedule
+// over the L - CB local bits.  Couplings that reach a CTA bit read the partner
+// block from the peer CTA's shared memory (distributed shared memory); one
+// cluster barrier per Chebyshev order publishes T_n to the peers.  The
+// cluster holds 2C CTAs: ranks 0 .. C-1 the state, C .. 2C-1 the reference;
+// both run the same number of orders, so their barriers pair up.
+namespace cg = cooperative_groups;
+
+template <typename T>
+__device__ __forceinline__ T* peer_ptr(cg::cluster_group& cl, T* local, unsigned rank, unsigned mine) {
+  return rank == mine ? local : cl.map_shared_rank(local, rank);
+}
+
+template <int L, int R, int CB, typename Real>
+__device__ void evolve_dist(const Args& args, const Smem<Real>& sm, const RealDev& rd, double2* st,
+                            const Op& op, const TypeDev& ty, int vec, uint32_t part,
+                            cg::cluster_group& cl, double* s_norm) {
+  constexpr int Ll = L - CB;
+  constexpr int C = 1 << CB;
+  using Gm = Geo<Ll, R>;
+  using C2 = typename Cplx<Real>::T;
+  constexpr int NT = Gm::NT, NA = Gm::NA, G = Gm::G;
+  constexpr uint32_t N = 1u << L;
+  constexpr int bl = Gm::base(G - 1);
+  constexpr bool kMixed = std::is_same<Real, float>::value;
+  const uint32_t t = threadIdx.x;
+  const unsigned me = cl.block_rank();
+  const unsigned group = static_cast<unsigned>(vec) * C;
+  const uint32_t hi = part << Ll;
+  const int P = rd.npairs;
+  const double* cb = args.cpool + ty.c_off;
+  const int2* pl = args.pairs + rd.pair_off;
+
+  __syncthreads();
+  for (int i = t; i < L * L; i += NT) {
+    sm.cff[i] = Real(0);
+    sm.cfb[i] = Real(0);
+  }
+  __syncthreads();
+  for (int p = t; p < P; p += NT) {
+    const int2 q = pl[p];
+    sm.cff[q.x * L + q.y] = Real(cb[p]);
+    sm.cfb[q.x * L + q.y] = Real(cb[P + p]);
+  }
+  for (int s = t; s < L; s += NT) {
+    sm.ccx[s] = Real(cb[3 * P + L + s]);
+    sm.ccy[s] = Real(cb[3 * P + 2 * L + s]);
+  }
+  if (t == 0) {
+    int nc = 0;
+    if (kMixed) {
+      const double* ct = cb + 3 * P + 3 * L;
+      for (int c = 0; c < kCorr; ++c) {
+        const int pi = static_cast<int>(ct[4 * c]);
+        if (pi < 0) continue;
+        const int2 q = pl[pi];
+        sm.corr_mask[nc] = make_uint2(1u << q.x, 1u << q.y);
+        sm.corr_coef[nc] = make_double2(ct[4 * c + 1], ct[4 * c + 2]);
+        ++nc;
+      }
+    }
+    *sm.corr_n = nc;
+  }
+  double dg[NA];
+#pragma unroll
+  for (int a = 0; a < NA; ++a) {
+    const uint32_t k = hi | t | (uint32_t(a) << bl);
+    double d = 0.0;
+    for (int s = 0; s < L; ++s) {
+      const double c = cb[3 * P + s];
+      d += ((k >> s) & 1u) ? c : -c;
+    }
+    for (int p = 0; p < P; ++p) {
+      const int2 q = pl[p];
+      const double c = cb[2 * P + p];
+      d += (((k >> q.x) ^ (k >> q.y)) & 1u) ? -c : c;
+    }
+    dg[a] = ty.scale * d;
+  }
+  __syncthreads();
+
+  const bool has_trans = (ty.flags & 1) != 0, has_fb = (ty.flags & 2) != 0;
+  const int ncorr = *sm.corr_n;
+  const double2* wts = args.wpool + ty.w_off;
+  const double a0 = wts[0].x;
+  double2* psig = st + vec * N;
+  // CTA-bit fields and CTA-CTA couplings, uniform over this CTA
+  Real tcx[CB > 0 ? CB : 1], tcy[CB > 0 ? CB : 1];
+#pragma unroll
+  for (int jb = 0; jb < CB; ++jb) {
+    tcx[jb] = has_trans ? sm.ccx[Ll + jb] : Real(0);
+    tcy[jb] = has_trans ? (((part >> jb) & 1u) ? -sm.ccy[Ll + jb] : sm.ccy[Ll + jb]) : Real(0);
+  }
+  constexpr int NCC = CB * (CB - 1) / 2;
+  Real ccc[NCC > 0 ? NCC : 1];
+  uint32_t cmask[NCC > 0 ? NCC : 1];
+  {
+    int q = 0;
+#pragma unroll
+    for (int j1 = 0; j1 < CB; ++j1) {
+#pragma unroll
+      for (int j2 = j1 + 1; j2 < CB; ++j2) {
+        const bool anti = (((part >> j1) ^ (part >> j2)) & 1u) != 0;
+        ccc[q] = anti ? sm.cff[(Ll + j1) * L + Ll + j2] : (has_fb ? sm.cfb[(Ll + j1) * L + Ll + j2] : Real(0));
+        cmask[q] = (1u << j1) | (1u << j2);
+        ++q;
+      }
+    }
+  }
+
+  for (int step = 0; step < op.b; ++step) {
+    int ic = 0;  // which of buf[0], buf[1] holds T_{n-1}
+#pragma unroll
+    for (int a = 0; a < NA; ++a) {
+      const uint32_t kl = t | (uint32_t(a) << bl);
+      double2 p = __ldcg(&psig[hi | kl]);
+      C2 c;
+      c.x = Real(p.x);
+      c.y = Real(p.y);
+      sm.buf[0][pad<R>(kl)] = c;
+      p.x *= a0;
+      p.y *= a0;
+      __stcg(&psig[hi | kl], p);
+    }
+    cl.sync();  // every slice of T_0 is in place
+    for (int n = 1; n <= ty.order; ++n) {
+      const double2 cn = wts[n];
+      C2* cur = sm.buf[ic];
+      C2* prv = sm.buf[ic ^ 1];
+      const C2* rc[CB > 0 ? CB : 1];
+#pragma unroll
+      for (int jb = 0; jb < CB; ++jb) rc[jb] = cl.map_shared_rank(cur, group + (part ^ (1u << jb)));
+      front_layouts<Ll, R, Real, 0, L, CB>(sm, cur, t, has_trans, has_fb, rc, part);
+      C2 acc[NA], own[NA];
+      layout_pass<Ll, R, Real, G - 1, L, CB>(sm, cur, acc, own, t, has_trans, has_fb, rc, part);
+      C2* prv_mine = prv + pad<R>(t);
+#pragma unroll
+      for (int a = 0; a < NA; ++a) {
+        const uint32_t kl = t | (uint32_t(a) << bl);
+        const uint32_t off = pad<R>(kl);
+#pragma unroll
+        for (int jb = 0; jb < CB; ++jb) {
+          if (has_trans) {
+            const C2 w = rc[jb][off];
+            acc[a].x += tcx[jb] * w.x - tcy[jb] * w.y;
+            acc[a].y += tcx[jb] * w.y + tcy[jb] * w.x;
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < NCC; ++q) {
+          const C2 w = cl.map_shared_rank(cur, group + (part ^ cmask[q]))[off];
+          acc[a].x += ccc[q] * w.x;
+          acc[a].y += ccc[q] * w.y;
+        }
+        const uint32_t k = hi | kl;
+        double hx = double(acc[a].x) + dg[a] * double(own[a].x);
+        double hy = double(acc[a].y) + dg[a] * double(own[a].y);
+#pragma unroll
+        for (int c = 0; c < kCorr; ++c) {
+          if (c < ncorr) {
+            const uint2 mk = sm.corr_mask[c];
+            const double2 cc = sm.corr_coef[c];
+            const uint32_t kp = k ^ mk.x ^ mk.y;
+            const C2 w = peer_ptr(cl, cur, group + (kp >> Ll), me)[pad<R>(kp & ((1u << Ll) - 1u))];
+            const double co = (((k & mk.x) != 0) == ((k & mk.y) != 0)) ? cc.y : cc.x;
+            hx += co * double(w.x);
+            hy += co * double(w.y);
+          }
+        }
+        const uint32_t offs = pad<R>(uint32_t(a) << bl);
+        if (n == 1) {
+          hx *= 0.5;
+          hy *= 0.5;
+        } else {
+          const C2 q = prv_mine[offs];
+          hx -= double(q.x);
+          hy -= double(q.y);
+        }
+        C2 tn;
+        tn.x = Real(hx);
+        tn.y = Real(hy);
+        prv_mine[offs] = tn;
+        double2 p = __ldcg(&psig[k]);
+        p.x += cn.x * hx - cn.y * hy;
+        p.y += cn.x * hy + cn.y * hx;
+        __stcg(&psig[k], p);
+      }
+      cl.sync();  // T_n published; every peer is done reading T_{n-1}
+      ic ^= 1;
+    }
+    if (op.c) {  // autonormalise over the C CTAs of this vector, in part order
+      double s = 0.0;
+#pragma unroll
+      for (int a = 0; a < NA; ++a) {
+        const double2 p = __ldcg(&psig[hi | t | (uint32_t(a) << bl)]);
+        s += p.x * p.x + p.y * p.y;
+      }
+      s = cta_sum2<NT>(make_double2(s, 0.0), sm.red).x;
+      if (t == 0) *s_norm = s;
+      cl.sync();
+      double tot = 0.0;
+      for (int q = 0; q < C; ++q) tot += *peer_ptr(cl, s_norm, group + q, me);
+      const double nrm = sqrt(tot);
+      if (nrm == 0.0 || !isfinite(nrm)) {
+        if (t == 0 && part == 0) atomicExch(args.flags, nrm == 0.0 ? SS_ERR_DOMAIN : SS_ERR_NUMERIC);
+      } else {
+        const double f = 1.0 / nrm;
+#pragma unroll
+        for (int a = 0; a < NA; ++a) {
+          const uint32_t k = hi | t | (uint32_t(a) << bl);
+          double2 p = __ldcg(&psig[k]);
+          p.x *= f;
+          p.y *= f;
+          __stcg(&psig[k], p);
+        }
+      }
+      cl.sync();  // s_norm may be reused
+    }
+  }
+}
+
+// A pulse on a vector spread over C CTAs: each CTA rotates a slice of the
+// amplitude pairs of every target spin, a cluster barrier between spins.
+template <int NT, int C>
+__device__ void pulse_dist(const Args& args, int L, double2* st, const Op& op, int vec,
+                           uint32_t part, long long rot_off, cg::cluster_group& cl) {
+  const double* u = args.rots + rot_off + 8 * op.a;
+  const double llr = u[0], lli = u[1], lhr = u[2], lhi = u[3];
+  const double hlr = u[4], hli = u[5], hhr = u[6], hhi = u[7];
+  const uint32_t n = 1u << L;
+  const uint32_t slice = (n / 2) / C;
+  const int s0 = op.b < 0 ? 0 : op.b, s1 = op.b < 0 ? L : op.b + 1;
+  double2* psi = st + vec * n;
+  for (int s = s0; s < s1; ++s) {
+    const uint32_t low = (1u << s) - 1u;
+    for (uint32_t j = part * slice + threadIdx.x; j < (part + 1) * slice; j += NT) {
+      const uint32_t lo = ((j & ~low) << 1) | (j & low);
+      const uint32_t hi = lo | (1u << s);
+      const double2 a = __ldcg(&psi[lo]), b = __ldcg(&psi[hi]);
+      __stcg(&psi[lo], make_double2((llr * a.x - lli * a.y) + (lhr * b.x - lhi * b.y),
+                                    (llr * a.y + lli * a.x) + (lhr * b.y + lhi * b.x)));
+      __stcg(&psi[hi], make_double2((hlr * a.x - hli * a.y) + (hhr * b.x - hhi * b.y),
+                                    (hlr * a.y + hli * a.x) + (hhr * b.y + hhi * b.x)));
+    }
+    __threadfence();
+    cl.sync();
+  }
+}
+
+// Observables of a realisation whose vectors live in global memory, the
+// amplitude range split over the cluster's CTAs; rank 0 adds the per-CTA
+// partial sums in rank order and writes the row.
+template <int NT>
+__device__ void measure_dist(const Args& args, double2* red, double2* s_part, const RealDev& rd,
+                             const double2* st, const Op& op, cg::cluster_group& cl) {
+  const int L = rd.L;
+  const uint32_t N = 1u << L;
+  const unsigned me = cl.block_rank(), nb = cl.num_blocks();
+  const uint32_t chunk = N / nb;
+  const uint32_t k0 = me * chunk, k1 = k0 + chunk;
+  const uint32_t t = threadIdx.x;
+  const double2* psi = st;
+  const double2* ref = st + N;
+  for (int i = 0; i < args.nobs; ++i) {
+    const int kind = args.obs[3 * i], axis = args.obs[3 * i + 1], spin = args.obs[3 * i + 2];
+    double2 v = make_double2(0.0, 0.0);
+    if (kind == SS_OBS_CORR) {
+      for (uint32_t k = k0 + t; k < k1; k += NT) {
+        double sr = 0.0, si = 0.0;
+        for (int s = 0; s < L; ++s) {
+          const double2 q = sigma_at(psi, k, s, axis);
+          sr += q.x;
+          si += q.y;
+        }
+        const double2 r = ref[k];
+        v.x += r.x * sr + r.y * si;
+        v.y += r.x * si - r.y * sr;
+      }
+    } else if (kind == SS_OBS_MAG) {
+      for (uint32_t k = k0 + t; k < k1; k += NT) {
+        const double2 q = sigma_at(psi, k, spin, axis);
+        const double2 p = psi[k];
+        v.x += p.x * q.x + p.y * q.y;
+      }
+    } else if (kind == SS_OBS_NORM) {
+      for (uint32_t k = k0 + t; k < k1; k += NT) {
+        const double2 p = psi[k], r = ref[k];
+        v.x += p.x * p.x + p.y * p.y;
+        v.y += r.x * r.x + r.y * r.y;
+      }
+    } else {
+      const TypeDev ty = args.types[rd.type_off + args.measure_type];
+      const double* cb = args.cpool + ty.c_off;
+      const int2* pl = args.pairs + rd.pair_off;
+      const int P = rd.npairs;
+      for (uint32_t k = k0 + t; k < k1; k += NT) {
+        const double2 p = psi[k];
+        double d = 0.0;
+        for (int s = 0; s < L; ++s) d += ((k >> s) & 1u) ? cb[3 * P + s] : -cb[3 * P + s];
+        for (int q = 0; q < P; ++q) {
+          const int2 pr = pl[q];
+          d += (((k >> pr.x) ^ (k >> pr.y)) & 1u) ? -cb[2 * P + q] : cb[2 * P + q];
+        }
+        double hr = d * p.x, hi = d * p.y;
+        for (int s = 0; s < L; ++s) {
+          const double cx = cb[3 * P + L + s];
+          const double cy = ((k >> s) & 1u) ? -cb[3 * P + 2 * L + s] : cb[3 * P + 2 * L + s];
+          const double2 w = psi[k ^ (1u << s)];
+          hr += cx * w.x - cy * w.y;
+          hi += cx * w.y + cy * w.x;
+        }
+        for (int q = 0; q < P; ++q) {
+          const int2 pr = pl[q];
+          const bool anti = (((k >> pr.x) ^ (k >> pr.y)) & 1u) != 0;
+          const double c = anti ? cb[q] : cb[P + q];
+          const double2 w = psi[k ^ (1u << pr.x) ^ (1u << pr.y)];
+          hr += c * w.x;
+          hi += c * w.y;
+        }
+        v.x += hr * p.x + hi * p.y;
+      }
+    }
+    v = cta_sum2<NT>(v, red);
+    if (t == 0) s_part[i] = v;
+  }
+  cl.sync();
+  if (me == 0 && t == 0) {
+    double* row = args.rows + rd.row_off + static_cast<long long>(op.a) * args.width;
+    int col = 0;
+    for (int i = 0; i < args.nobs; ++i) {
+      const int kind = args.obs[3 * i];
+      double2 v = make_double2(0.0, 0.0);
+      for (unsigned b = 0; b < nb; ++b) v += *peer_ptr(cl, &s_part[i], b, me);
+      if (kind == SS_OBS_CORR) {
+        row[col] = v.x;
+        row[col + 1] = v.y;
+      } else if (kind == SS_OBS_NORM) {
+        row[col] = sqrt(v.x);
+        row[col + 1] = sqrt(v.y);
+      } else {
+        row[col] = v.x;
+      }
+      col += (kind == SS_OBS_CORR || kind == SS_OBS_NORM) ? 2 : 1;
+    }
+  }
+  cl.sync();  // partial slots may be reused
+}
+
+constexpr int kMaxDistObs = 8;
+
+template <int L, int R, int CB, typename Real>
+struct DistLayout {
+  static constexpr int Ll = L - CB;
+  using SL = SmemLayout<Ll, R, Real, PSI_GLOBAL>;
+  // the coupling tables cover all L spins
+  static constexpr size_t NP = SL::NP;
+  using C2 = typename Cplx<Real>::T;
+  static constexpr size_t bufs = 3 * NP * sizeof(C2);
+  static constexpr size_t at_coef = bufs;
+  static constexpr size_t coef = (2 * L * L + 2 * L) * sizeof(Real);
+  static constexpr size_t at_corr = (at_coef + coef + 15) & ~size_t{15};
+  static constexpr size_t corr = kCorr * (sizeof(uint2) + sizeof(double2)) + 16;
+  static constexpr size_t at_red = (at_corr + corr + 15) & ~size_t{15};
+  static constexpr size_t at_part = at_red + 32 * sizeof(double2);
+  static constexpr size_t at_norm = at_part + kMaxDistObs * sizeof(double2);
+  static constexpr size_t total = at_norm + 16;
+};
+
+// One realisation per cluster of 2 * 2^CB CTAs (cluster size given at launch).
+template <int L, int R, int CB, typename Real>
+__global__ void __launch_bounds__(Geo<L - CB, R>::NT) k_batch_dist(const __grid_constant__ Args args) {
+  constexpr int Ll = L - CB, C = 1 << CB;
+  using Gm = Geo<Ll, R>;
+  using C2 = typename Cplx<Real>::T;
+  using DL = DistLayout<L, R, CB, Real>;
+  constexpr int NT = Gm::NT, NP = static_cast<int>(DL::NP);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Smem<Real> sm;
+  C2* base = reinterpret_cast<C2*>(smem_raw);
+  sm.buf[0] = base;
+  sm.buf[1] = base + NP;
+  sm.buf[2] = base + 2 * NP;
+  sm.psi = nullptr;
+  Real* coef = reinterpret_cast<Real*>(smem_raw + DL::at_coef);
+  sm.cff = coef;
+  sm.cfb = coef + L * L;
+  sm.ccx = coef + 2 * L * L;
+  sm.ccy = coef + 2 * L * L + L;
+  sm.corr_coef = reinterpret_cast<double2*>(smem_raw + DL::at_corr);
+  sm.corr_mask = reinterpret_cast<uint2*>(smem_raw + DL::at_corr + kCorr * sizeof(double2));
+  sm.corr_n = reinterpret_cast<int*>(smem_raw + DL::at_corr + kCorr * (sizeof(double2) + sizeof(uint2)));
+  sm.red = reinterpret_cast<double2*>(smem_raw + DL::at_red);
+  double2* s_part = reinterpret_cast<double2*>(smem_raw + DL::at_part);
+  double* s_norm = reinterpret_cast<double*>(smem_raw + DL::at_norm);
+  __shared__ int s_work;
+  cg::cluster_group cluster = cg::this_cluster();
+  const unsigned rank = cluster.block_rank();
+  const int vec = static_cast<int>(rank / C);
+  const uint32_t part = rank % C;
+  int* lead_work = cluster.map_shared_rank(&s_work, 0);
+
+  for (;;) {
+    if (rank == 0 && threadIdx.x == 0) s_work = static_cast<int>(atomicAdd(args.counter, 1u));
+    cluster.sync();
+    const int w = *lead_work;
+    cluster.sync();
+    if (w >= args.nwork) break;
+    const RealDev rd = args.reals[args.work[w]];
+    double2* st = args.states + rd.state_off;
+    for (int i = args.op_begin; i < args.op_end; ++i) {
+      const Op op = args.ops[i];
+      if (op.kind == OP_EVOLVE) {
+        const TypeDev ty = args.types[rd.type_off + op.a];
+        if (ty.order > 0 && op.b > 0) {
+          evolve_dist<L, R, CB, Real>(args, sm, rd, st, op, ty, vec, part, cluster, s_norm);
+          __threadfence();
+          cluster.sync();  // psi complete in global memory
+        }
+      } else if (op.kind == OP_PULSE) {
+        pulse_dist<NT, C>(args, L, st, op, vec, part, rd.rot_off, cluster);
+      } else {
+        __threadfence();
+        cluster.sync();
+        measure_dist<NT>(args, sm.red, s_part, rd, st, op, cluster);
+      }
+    }
+  }
+}
+
 // ------------------------------------------------------------ variants
 struct Variant {
   int L, R;
@@ -450,12 +882,20 @@ struct Variant {
   int threads;
   size_t smem;
   void (*kernel)(Args);
+  int cb;  // each vector spread over 2^cb CTAs (k_batch_dist); 0 = one CTA
+  int cluster() const { return 2 << cb; }
 };
 
 template <int L, int R, typename Real, int PSI>
 Variant make_variant() {
   return Variant{L, R, std::is_same<Real, float>::value, PSI, Geo<L, R>::NT,
-                 SmemLayout<L, R, Real, PSI>::total, &k_batch<L, R, Real, PSI>};
+                 SmemLayout<L, R, Real, PSI>::total, &k_batch<L, R, Real, PSI>, 0};
+}
+
+template <int L, int R, int CB, typename Real>
+Variant make_dist_variant() {
+  return Variant{L, R, std::is_same<Real, float>::value, PSI_GLOBAL, Geo<L - CB, R>::NT,
+                 DistLayout<L, R, CB, Real>::total, &k_batch_dist<L, R, CB, Real>, CB};
 }
 
 // The per-size schedules: register bits R and where psi lives.  Chosen so a
@@ -471,6 +911,10 @@ const std::vector<Variant>& variants() {
       make_variant<8, 3, double, PSI_REG>(),    make_variant<9, 3, double, PSI_SMEM>(),
       make_variant<10, 3, double, PSI_SMEM>(),  make_variant<11, 3, double, PSI_SMEM>(),
       make_variant<12, 3, double, PSI_GLOBAL>(),
+      // vectors over clusters: 2 / 4 / 8 CTAs per vector
+      make_dist_variant<14, 4, 1, float>(),     make_dist_variant<15, 4, 2, float>(),
+      make_dist_variant<16, 4, 3, float>(),     make_dist_variant<13, 3, 1, double>(),
+      make_dist_variant<14, 3, 2, double>(),    make_dist_variant<15, 3, 3, double>(),
   };
   return v;
 }
@@ -939,7 +1383,7 @@ void build_plan(ss_batch* b, const ss_run_config& c) {
     bk.var = find_variant(L, mixed);
     if (!bk.var) {
       fail(SS_ERR_INVALID_ARGUMENT,
-           std::string("the batched engine covers L = 6..") + (mixed ? "13" : "12") +
+           std::string("the batched engine covers L = 6..") + (mixed ? "16" : "15") +
                " in this precision; got L = " + std::to_string(L));
     }
     std::stable_sort(list.begin(), list.end(),
@@ -957,16 +1401,30 @@ void build_plan(ss_batch* b, const ss_run_config& c) {
     SS_CUDA(cudaFuncSetAttribute(bk.var->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(bk.var->smem)));
     cudaLaunchConfig_t lc{};
-    lc.gridDim = dim3(2 * kClusterSize);
+    cudaLaunchAttribute attr[1];
     lc.blockDim = dim3(bk.var->threads);
     lc.dynamicSmemBytes = bk.var->smem;
+    if (bk.var->cb > 0) {
+      if (bk.var->cluster() > 8) {
+        SS_CUDA(cudaFuncSetAttribute(bk.var->kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+      }
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = static_cast<unsigned>(bk.var->cluster());
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      lc.attrs = attr;
+      lc.numAttrs = 1;
+      lc.gridDim = dim3(bk.var->cluster());
+    } else {
+      lc.gridDim = dim3(2 * kClusterSize);
+    }
     int resident = 0;
     SS_CUDA(cudaOccupancyMaxActiveClusters(&resident, bk.var->kernel, &lc));
     require(resident > 0, SS_ERR_RUNTIME, "batched kernel cluster does not fit the device");
     const double share = total_weight > 0.0 ? weight[i] / total_weight : 1.0;
     int clusters = static_cast<int>(share * resident);
     clusters = std::max(1, std::min<int>(clusters, static_cast<int>(bk.work.size())));
-    bk.grid = kClusterSize * clusters;
+    bk.grid = (bk.var->cb > 0 ? bk.var->cluster() : kClusterSize) * clusters;
   }
 }
 
@@ -1012,7 +1470,24 @@ void capture(ss_batch* b) {
       a.width = static_cast<int>(b->width);
       a.measure_type = b->ntypes;
       a.flags = b->d_flags;
-      bk.var->kernel<<<bk.grid, bk.var->threads, bk.var->smem, ks>>>(a);
+      if (bk.var->cb > 0) {
+        // vectors over clusters: the cluster size is a launch attribute
+        cudaLaunchConfig_t lc{};
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = static_cast<unsigned>(bk.var->cluster());
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        lc.gridDim = dim3(bk.grid);
+        lc.blockDim = dim3(bk.var->threads);
+        lc.dynamicSmemBytes = bk.var->smem;
+        lc.stream = ks;
+        lc.attrs = attr;
+        lc.numAttrs = 1;
+        SS_CUDA(cudaLaunchKernelEx(&lc, bk.var->kernel, a));
+      } else {
+        bk.var->kernel<<<bk.grid, bk.var->threads, bk.var->smem, ks>>>(a);
+      }
       SS_CUDA(cudaGetLastError());
       ++launches;
       if (i > 0) {

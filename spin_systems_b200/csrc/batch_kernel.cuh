@@ -199,11 +199,21 @@ __device__ __forceinline__ double2 cta_sum2(double2 v, double2* red) {
 // One layout pass over the register group of layout g: couplings and fields
 // assigned to g are applied into acc.  For g > 0 acc is first loaded from the
 // partial buffer; own[] receives T_{n-1} of this thread's amplitudes.
-template <int L, int R, typename Real, int g>
+//
+// A vector spread over 2^CB CTAs of a cluster (see k_batch_dist) runs the same
+// layouts over its L local bits; LS is then the whole system's spin count (the
+// stride of the coupling tables) and spins L .. LS-1 are CTA bits.  A
+// coupling (b + p, j) with j a CTA bit is applied in the first layout holding
+// b + p, from the partner block at the same local offsets in the CTA across
+// bit j (rcur[j - L], distributed shared memory); `part` is this CTA's value
+// of the CTA bits.
+template <int L, int R, typename Real, int g, int LS = L, int CB = 0>
 __device__ __forceinline__ void layout_pass(const Smem<Real>& sm, const typename Cplx<Real>::T* cur,
                                             typename Cplx<Real>::T (&acc)[Geo<L, R>::NA],
                                             typename Cplx<Real>::T (&own)[Geo<L, R>::NA],
-                                            uint32_t t, bool has_trans, bool has_fb) {
+                                            uint32_t t, bool has_trans, bool has_fb,
+                                            const typename Cplx<Real>::T* const* rcur = nullptr,
+                                            uint32_t part = 0) {
   using Gm = Geo<L, R>;
   using C2 = typename Cplx<Real>::T;
   constexpr int b = Gm::base(g);
@@ -228,8 +238,8 @@ __device__ __forceinline__ void layout_pass(const Smem<Real>& sm, const typename
 #pragma unroll
     for (int q = p + 1; q < R; ++q) {
       if (Gm::pair_layout(b + p, b + q) == g) {
-        const Real ff = sm.cff[(b + p) * L + (b + q)];
-        const Real fb = sm.cfb[(b + p) * L + (b + q)];
+        const Real ff = sm.cff[(b + p) * LS + (b + q)];
+        const Real fb = sm.cfb[(b + p) * LS + (b + q)];
 #pragma unroll
         for (int a = 0; a < NA; ++a) {
           const int src = a ^ (1 << p) ^ (1 << q);
@@ -273,8 +283,8 @@ __device__ __forceinline__ void layout_pass(const Smem<Real>& sm, const typename
 #pragma unroll
     for (int p = 0; p < R; ++p) {
       const bool mine = Gm::cross_mine(g, p);
-      const Real ff = mine ? sm.cff[(b + p) * L + j] : Real(0);
-      const Real fb = mine ? sm.cfb[(b + p) * L + j] : Real(0);
+      const Real ff = mine ? sm.cff[(b + p) * LS + j] : Real(0);
+      const Real fb = mine ? sm.cfb[(b + p) * LS + j] : Real(0);
       c0[p] = bj ? ff : fb;  // register bit clear: aligned iff bit j clear
       c1[p] = bj ? fb : ff;  // register bit set
     }
@@ -292,6 +302,37 @@ __device__ __forceinline__ void layout_pass(const Smem<Real>& sm, const typename
       }
     }
   }
+
+  // Couplings (b + p, L + jb) with a CTA bit: the partner block is this
+  // thread's own block in the CTA across bit jb.
+  if constexpr (CB > 0) {
+#pragma unroll 1
+    for (int jb = 0; jb < CB; ++jb) {
+      const int j = L + jb;
+      const bool bj = ((part >> jb) & 1u) != 0;
+      Real c0[R], c1[R];
+#pragma unroll
+      for (int p = 0; p < R; ++p) {
+        const bool mine = Gm::first_layout(b + p) == g;
+        const Real ff = mine ? sm.cff[(b + p) * LS + j] : Real(0);
+        const Real fb = mine ? sm.cfb[(b + p) * LS + j] : Real(0);
+        c0[p] = bj ? ff : fb;
+        c1[p] = bj ? fb : ff;
+      }
+      const C2* partner = rcur[jb] + pad<R>(kb);
+#pragma unroll
+      for (int x = 0; x < NA; ++x) {
+        const C2 v = partner[pad<R>(uint32_t(x) << b)];
+#pragma unroll
+        for (int p = 0; p < R; ++p) {
+          const int dst = x ^ (1 << p);
+          const Real c = ((dst >> p) & 1) ? c1[p] : c0[p];
+          acc[dst].x += c * v.x;
+          acc[dst].y += c * v.y;
+        }
+      }
+    }
+  }
 }
 
 template <int L, int R, typename Real, int g>
@@ -306,15 +347,17 @@ __device__ __forceinline__ void store_partial(const Smem<Real>& sm,
 }
 
 // Layouts 0 .. G-2, each followed by a barrier.
-template <int L, int R, typename Real, int g>
+template <int L, int R, typename Real, int g, int LS = L, int CB = 0>
 __device__ __forceinline__ void front_layouts(const Smem<Real>& sm, const typename Cplx<Real>::T* cur,
-                                              uint32_t t, bool has_trans, bool has_fb) {
+                                              uint32_t t, bool has_trans, bool has_fb,
+                                              const typename Cplx<Real>::T* const* rcur = nullptr,
+                                              uint32_t part = 0) {
   if constexpr (g < Geo<L, R>::G - 1) {
     typename Cplx<Real>::T acc[Geo<L, R>::NA], own[Geo<L, R>::NA];
-    layout_pass<L, R, Real, g>(sm, cur, acc, own, t, has_trans, has_fb);
+    layout_pass<L, R, Real, g, LS, CB>(sm, cur, acc, own, t, has_trans, has_fb, rcur, part);
     store_partial<L, R, Real, g>(sm, acc, t);
     __syncthreads();
-    front_layouts<L, R, Real, g + 1>(sm, cur, t, has_trans, has_fb);
+    front_layouts<L, R, Real, g + 1, LS, CB>(sm, cur, t, has_trans, has_fb, rcur, part);
   }
 }
 

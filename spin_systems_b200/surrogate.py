@@ -1,0 +1,269 @@
+"""Learned echo surrogate: a network from sweep parameters to the
+disorder-averaged S^x echo, trained on curves the batched engine generates,
+judged by the exact propagator, which is also its fallback.
+
+Parameter space (one point = one experiment, averaged over realisations):
+  areal density rho in [0.5, 2]   -> dipolar_scale = rho^(3/2) (lengths scale
+                                     as rho^(-1/2), couplings as r^-3)
+  field sigma in [0, 1.5]         -> Gaussian Hz disorder
+  tau in [0.05, 1]                -> pulse spacing
+  pulse-angle error e in [-0.05, 0.05] -> every pulse angle times (1 + e)
+  sequence in {CPMG, XY-8}        -> pi/2_x, then 128 echoes:
+                                     CPMG (tau, pi_y, tau, measure) x 128,
+                                     XY-8 (tau/2, pi_a, tau/2, measure) for
+                                     a in X Y X Y Y X Y X, x 16
+  L in {10, 12, 14}
+The target is the realisation average of Re corr_x(t) / ||ref||^2 at the 128
+measurement times, with every point seeing the same realisations (seed
+20240726, indices 0 .. R-1), so the average is a smooth function of the
+continuous parameters.
+
+Network: 6 -> 256 -> 256 -> 256 -> 128 GELU (ss_mlp_*), BF16 weights and
+activations, FP32 accumulation, trained with Adam by the library's tcgen05
+kernels.  The error model for the fallback is empirical: the error of a
+query is estimated as the largest error of its nearest held-out calibration
+points (same sequence and L), times a safety factor; a query whose estimate
+exceeds the tolerance (1e-3 by default) is answered by the exact propagator.
+
+The reference has no learned component and no sweep driver; its parameter
+sweeps are separate runs of io/Experiment.cpp:57-72.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import time
+from pathlib import Path
+from typing import Callable, Optional
+
+import numpy as np
+
+from . import Batch, Engine, Mlp, abi
+from .abi import AXES3, Evolve, Measure, Pulse, Repeat, RunSpec
+
+SEED = 20240726
+RANGES = {"density": (0.5, 2.0), "sigma": (0.0, 1.5), "tau": (0.05, 1.0),
+          "angle_error": (-0.05, 0.05)}
+SEQUENCES = ("cpmg", "xy8")
+SIZES = (10, 12, 14)
+POINTS = 128
+PARAMS = np.dtype([("density", "f8"), ("sigma", "f8"), ("tau", "f8"), ("angle_error", "f8"),
+                   ("sequence", "i4"), ("nspins", "i4")])
+
+
+def sample(n: int, seed: int, sizes=SIZES, sequences=(0, 1), ranges=None) -> np.ndarray:
+    """n points drawn uniformly from the parameter space."""
+    rng = np.random.default_rng(seed)
+    r = dict(RANGES, **(ranges or {}))
+    p = np.zeros(n, dtype=PARAMS)
+    for k in ("density", "sigma", "tau", "angle_error"):
+        lo, hi = r[k]
+        p[k] = rng.uniform(lo, hi, n)
+    p["sequence"] = rng.choice(np.asarray(sequences), n)
+    p["nspins"] = rng.choice(np.asarray(sizes), n)
+    return p
+
+
+def features(p: np.ndarray) -> np.ndarray:
+    """Network inputs in [-1, 1]: the four continuous parameters over their
+    full ranges, the sequence as -1 / +1 and L as (L - 12) / 2."""
+    x = np.zeros((len(p), 6), dtype=np.float32)
+    for i, k in enumerate(("density", "sigma", "tau", "angle_error")):
+        lo, hi = RANGES[k]
+        x[:, i] = 2.0 * (p[k] - lo) / (hi - lo) - 1.0
+    x[:, 4] = 2.0 * p["sequence"] - 1.0
+    x[:, 5] = (p["nspins"] - 12) / 2.0
+    return x
+
+
+def program(sequence: int, points: int = POINTS):
+    if sequence == 0:
+        body = [Evolve(1.0, tau_from_draw=True), Pulse(math.pi, AXES3["y"]),
+                Evolve(1.0, tau_from_draw=True), Measure()]
+        return [Pulse(0.5 * math.pi, AXES3["x"]), Repeat(points, body)]
+    body = []
+    for a in "XYXYYXYX":
+        body += [Evolve(0.5, tau_from_draw=True), Pulse(math.pi, AXES3[a.lower()]),
+                 Evolve(0.5, tau_from_draw=True), Measure()]
+    return [Pulse(0.5 * math.pi, AXES3["x"]), Repeat(points // 8, body)]
+
+
+def sweep_spec(sequence: int, nspins: int, rows, realizations: int,
+               mixed_order_limit: int = 0) -> RunSpec:
+    return RunSpec(nspins=nspins, steps=program(sequence), observables=["corr:x", "norm"],
+                   realizations=realizations, seed=SEED, reference_axis="x",
+                   sweep=rows, mixed_order_limit=mixed_order_limit)
+
+
+def exact(engine: Engine, p: np.ndarray, realizations: int, precision: int = abi.MIXED,
+          max_batch: int = 32768, mixed_order_limit: int = 0) -> np.ndarray:
+    """The exact propagator's disorder-averaged echo [n][128] for each point,
+    run as batched sweeps (one batch per sequence and L, chunked)."""
+    out = np.zeros((len(p), POINTS))
+    per_batch = max(1, max_batch // realizations)
+    for seq in np.unique(p["sequence"]):
+        for L in np.unique(p["nspins"]):
+            idx = np.flatnonzero((p["sequence"] == seq) & (p["nspins"] == L))
+            for at in range(0, len(idx), per_batch):
+                sel = idx[at:at + per_batch]
+                rows = [(float(q["density"]) ** 1.5, float(q["sigma"]), float(q["tau"]),
+                         1.0 + float(q["angle_error"])) for q in p[sel]]
+                spec = sweep_spec(int(seq), int(L), rows, realizations, mixed_order_limit)
+                cfg = spec.config()
+                b = Batch(engine, cfg, 0, len(sel) * realizations, precision)
+                _, r = b.run()
+                b._destroy()
+                echo = r[:, :, 0] / (r[:, :, 3] ** 2)
+                out[sel] = echo.reshape(len(sel), realizations, POINTS).mean(axis=1)
+    return out
+
+
+def nearest_neighbour(train_p: np.ndarray, train_y: np.ndarray, query: np.ndarray) -> np.ndarray:
+    """The method without a network: the closest precomputed curve (feature
+    distance, same sequence and L)."""
+    fx, fq = features(train_p), features(query)
+    out = np.zeros((len(query), POINTS))
+    for i in range(len(query)):
+        same = (train_p["sequence"] == query["sequence"][i]) & (train_p["nspins"] == query["nspins"][i])
+        cand = np.flatnonzero(same)
+        if len(cand) == 0:
+            cand = np.arange(len(train_p))
+        d = ((fx[cand, :4] - fq[i, :4]) ** 2).sum(axis=1)
+        out[i] = train_y[cand[int(np.argmin(d))]]
+    return out
+
+
+class Surrogate:
+    """The trained network plus its empirical error model."""
+
+    def __init__(self, engine: Engine, batch: int = 1024, seed: int = 0):
+        self.engine = engine
+        self.net = Mlp(engine, batch=batch, seed=seed)
+        self.cal_x: Optional[np.ndarray] = None
+        self.cal_p: Optional[np.ndarray] = None
+        self.cal_err: Optional[np.ndarray] = None
+
+    def fit(self, p: np.ndarray, y: np.ndarray, steps: int, lr_start: float = 2e-3,
+            lr_end: float = 1e-5, seed: int = 0) -> np.ndarray:
+        self.net.set_data(features(p), np.asarray(y, dtype=np.float32))
+        return self.net.train(steps, lr_start, lr_end, seed)
+
+    def raw(self, p: np.ndarray) -> np.ndarray:
+        return self.net.forward(features(p)).astype(np.float64)
+
+    def calibrate(self, p: np.ndarray, y: np.ndarray) -> np.ndarray:
+        err = np.abs(self.raw(p) - y).max(axis=1)
+        self.cal_p, self.cal_x, self.cal_err = p.copy(), features(p), err
+        return err
+
+    def estimate_error(self, p: np.ndarray, k: int = 8, safety: float = 1.5) -> np.ndarray:
+        """Largest calibration error among the k nearest calibration points
+        (same sequence and L) times `safety`; +inf without calibration data."""
+        est = np.full(len(p), np.inf)
+        if self.cal_x is None:
+            return est
+        fq = features(p)
+        for i in range(len(p)):
+            same = np.flatnonzero((self.cal_p["sequence"] == p["sequence"][i]) &
+                                  (self.cal_p["nspins"] == p["nspins"][i]))
+            if len(same) == 0:
+                continue
+            d = ((self.cal_x[same, :4] - fq[i, :4]) ** 2).sum(axis=1)
+            near = same[np.argsort(d)[:k]]
+            est[i] = safety * self.cal_err[near].max()
+        return est
+
+    def predict(self, p: np.ndarray, fallback: Callable[[np.ndarray], np.ndarray],
+                tol: float = 1e-3):
+        """Curves for every point: the network where its estimated error is
+        within `tol`, the exact propagator (`fallback`) elsewhere.
+        Returns (curves, answered_by_network, estimated_error)."""
+        est = self.estimate_error(p)
+        use = est <= tol
+        out = np.zeros((len(p), POINTS))
+        if use.any():
+            out[use] = self.raw(p[use])
+        if (~use).any():
+            out[~use] = fallback(p[~use])
+        return out, use, est
+
+
+def run(args) -> dict:
+    """Generate, train, calibrate and judge; returns the report."""
+    eng = Engine(0)
+    rep: dict = {"realizations": args.realizations, "sizes": args.sizes, "steps": args.steps}
+    sizes = tuple(args.sizes)
+    ranges = {"tau": (args.tau_min, args.tau_max)}
+    n_train, n_cal, n_test = args.train, args.cal, args.test
+    p_all = sample(n_train + n_cal + n_test, args.seed, sizes=sizes, ranges=ranges)
+    t0 = time.perf_counter()
+    y_all = exact(eng, p_all, args.realizations, mixed_order_limit=-1)
+    gen_s = time.perf_counter() - t0
+    rep["generation"] = {"points": int(len(p_all)), "seconds": gen_s,
+                         "curves_per_s": len(p_all) * args.realizations / gen_s,
+                         "precision": "mixed, no FP64 routing"}
+    ptr, ytr = p_all[:n_train], y_all[:n_train]
+    pcal, ycal = p_all[n_train:n_train + n_cal], y_all[n_train:n_train + n_cal]
+    pte, yte = p_all[n_train + n_cal:], y_all[n_train + n_cal:]
+    sur = Surrogate(eng, batch=args.batch, seed=args.seed)
+    t0 = time.perf_counter()
+    losses = sur.fit(ptr, ytr, args.steps, args.lr, args.lr_end, seed=args.seed)
+    rep["training"] = {"seconds": time.perf_counter() - t0, "loss_first": float(losses[:10].mean()),
+                       "loss_last": float(losses[-50:].mean())}
+    cal_err = sur.calibrate(pcal, ycal)
+    t0 = time.perf_counter()
+    pred = sur.raw(pte)
+    inf_s = time.perf_counter() - t0
+    err = np.abs(pred - yte).max(axis=1)
+    nn = nearest_neighbour(ptr, ytr, pte)
+    nn_err = np.abs(nn - yte).max(axis=1)
+    rep["surrogate"] = {"test_points": int(len(pte)), "max_err_median": float(np.median(err)),
+                        "max_err_mean": float(err.mean()), "max_err_max": float(err.max()),
+                        "rms": float(np.sqrt(((pred - yte) ** 2).mean())),
+                        "inference_curves_per_s": len(pte) / inf_s,
+                        "calibration_err_median": float(np.median(cal_err))}
+    rep["nearest_neighbour"] = {"max_err_median": float(np.median(nn_err)),
+                                "max_err_mean": float(nn_err.mean()),
+                                "rms": float(np.sqrt(((nn - yte) ** 2).mean()))}
+    # The exact propagator's own rate on the test points (same realisations).
+    t0 = time.perf_counter()
+    exact(eng, pte, args.realizations, mixed_order_limit=-1)
+    ex_s = time.perf_counter() - t0
+    rep["exact_points_per_s"] = len(pte) / ex_s
+    rep["surrogate_speedup"] = (len(pte) / inf_s) / (len(pte) / ex_s)
+    for tol in (1e-3, 1e-2, 3e-2):
+        est = sur.estimate_error(pte)
+        use = est <= tol
+        viol = int(((err > tol) & use).sum())
+        rep[f"hybrid_tol_{tol:g}"] = {"answered_by_network": float(use.mean()), "violations": viol}
+    sur.net._destroy()
+    eng.close()
+    return rep
+
+
+def main(argv=None) -> None:
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--train", type=int, default=4096)
+    ap.add_argument("--cal", type=int, default=512)
+    ap.add_argument("--test", type=int, default=512)
+    ap.add_argument("--realizations", type=int, default=16)
+    ap.add_argument("--sizes", type=int, nargs="+", default=[10])
+    ap.add_argument("--tau-min", type=float, default=RANGES["tau"][0])
+    ap.add_argument("--tau-max", type=float, default=RANGES["tau"][1])
+    ap.add_argument("--steps", type=int, default=20000)
+    ap.add_argument("--batch", type=int, default=1024)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--lr-end", type=float, default=1e-5)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--out", type=str, default="")
+    args = ap.parse_args(argv)
+    rep = run(args)
+    text = json.dumps(rep, indent=1)
+    print(text)
+    if args.out:
+        Path(args.out).write_text(text + "\n")
+
+
+if __name__ == "__main__":
+    main()

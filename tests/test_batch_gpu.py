@@ -145,9 +145,9 @@ def test_mixed_order_limit_switches(engine):
     assert np.array_equal(every, fp64)
     spec.mixed_order_limit = -1
     assert (ss.Batch(engine, spec.config(), 0, 6, abi.MIXED).precisions() == abi.MIXED).all()
-    spec13 = workloads.xy8_finite(nspins=13, realizations=2, blocks=1)
-    spec13.mixed_order_limit = 1  # no FP64 kernel at L = 13: stays mixed
-    assert (ss.Batch(engine, spec13.config(), 0, 2, abi.MIXED).precisions() == abi.MIXED).all()
+    spec16 = workloads.xy8_finite(nspins=16, realizations=2, blocks=1)
+    spec16.mixed_order_limit = 1  # no FP64 kernel at L = 16: stays mixed
+    assert (ss.Batch(engine, spec16.config(), 0, 2, abi.MIXED).precisions() == abi.MIXED).all()
     assert (ss.Batch(engine, spec.config(), 0, 6, abi.FP64).precisions() == abi.FP64).all()
 
 

@@ -1,0 +1,50 @@
+"""Host logic of the learned echo surrogate (no GPU): the parameter space,
+network features, the pulse programs, the nearest-neighbour baseline and the
+fallback's error model."""
+import numpy as np
+
+from spin_systems_b200 import surrogate as sg
+
+
+def test_sample_and_features_cover_the_space():
+    p = sg.sample(2000, 3)
+    for k, (lo, hi) in sg.RANGES.items():
+        assert p[k].min() >= lo and p[k].max() <= hi
+    assert set(np.unique(p["nspins"])) == {10, 12, 14}
+    assert set(np.unique(p["sequence"])) == {0, 1}
+    x = sg.features(p)
+    assert x.shape == (2000, 6) and x.dtype == np.float32
+    assert x.min() >= -1.0 and x.max() <= 1.0
+    assert set(np.unique(x[:, 5])) == {-1.0, 0.0, 1.0}
+
+
+def test_programs_measure_128_times():
+    for seq in (0, 1):
+        spec = sg.sweep_spec(seq, 10, [(1.0, 0.5, 0.3, 1.0)], 4)
+        assert spec.measurement_count() == sg.POINTS
+        cfg = spec.config()
+        assert cfg.sweep_points == 1
+        assert [cfg.sweep_params[i] for i in range(4)] == [1.0, 0.5, 0.3, 1.0]
+
+
+def test_nearest_neighbour_returns_the_closest_curve_of_the_same_kind():
+    p = sg.sample(50, 1, sizes=(10, 12))
+    y = np.arange(50, dtype=float)[:, None] * np.ones((1, sg.POINTS))
+    q = p[[7, 21]].copy()
+    q["tau"] += 1e-6
+    got = sg.nearest_neighbour(p, y, q)
+    assert got[0, 0] == 7 and got[1, 0] == 21
+
+
+def test_error_model_takes_the_worst_near_calibration_point():
+    s = object.__new__(sg.Surrogate)
+    p = sg.sample(64, 2, sizes=(10,), sequences=(0,))
+    s.cal_p, s.cal_x = p, sg.features(p)
+    s.cal_err = np.full(64, 1e-4)
+    s.cal_err[5] = 5e-3
+    q = p[[5]].copy()
+    est = s.estimate_error(q, k=4, safety=1.0)
+    assert est[0] == 5e-3
+    far = p[[5]].copy()
+    far["nspins"] = 12
+    assert np.isinf(s.estimate_error(far)[0])
