@@ -209,6 +209,13 @@ def run_ours(args):
     eng = ss.Engine(local)
     stream = torch.cuda.ExternalStream(eng.stream, device=torch.device("cuda", local))
     first = rank * REALIZATIONS
+    tuned = []
+    if args.tune:
+        # The autotuner picks each kernel's schedule (mixed and the FP64
+        # routing target) on a sample of this rank's own realisations.
+        t0 = time.perf_counter()
+        tuned = ss.tune(eng, cfg, first, args.tune_sample, abi.MIXED)
+        tune_s = time.perf_counter() - t0
     batch = ss.Batch(eng, cfg, first, REALIZATIONS, abi.MIXED)
     stats = batch.stats()
     prec, amp_each = batch.work()
@@ -317,6 +324,9 @@ def run_ours(args):
                        "speedup_of_batched_mixed": value / world / plain_rate},
         "work": {"amplitude_orders_per_step": amp_orders, "orders_per_step": stats["orders"]},
         "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "schedule": ({"tuned": [{k: r[k] for k in ("L", "precision", "variant", "ns")} for r in tuned],
+                      "tuning_seconds": tune_s, "sample": args.tune_sample}
+                     if args.tune else {"tuned": [], "note": "default schedules (--no-tune)"}),
     }
     print(json.dumps(line), flush=True)
     barrier(world)
@@ -341,6 +351,10 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--tune", dest="tune", action="store_true", default=True,
+                    help="run the autotuner before timing (default)")
+    ap.add_argument("--no-tune", dest="tune", action="store_false")
+    ap.add_argument("--tune-sample", type=int, default=296)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference_arm(args)

@@ -334,6 +334,29 @@ int ss_batch_io_bytes(const ss_batch* batch, int64_t* h2d, int64_t* d2h);
 int ss_batch_precisions(const ss_batch* batch, int32_t* precision,
                         double* amplitude_orders);
 
+/* ------------------------------------------------------------- autotuner
+ * No counterpart in the reference (its CPU kernels have one schedule).
+ * Each batched size has candidate schedules -- register bits per thread
+ * (the term grouping of the layout passes) and CTAs per state vector.
+ * ss_batch_tune times every candidate of every size the config can draw
+ * (and, for SS_PRECISION_MIXED, the FP64 routing kernels) on `sample`
+ * realisations from `first` of the config's own program, installs the
+ * fastest in the process-wide schedule table keyed by device name, size and
+ * precision, and, if cache_path is not NULL, merges the table into that
+ * file (tab-separated text).  Later batches use the table's kernels and,
+ * when every size of a batch has been measured, the measured costs for
+ * their buckets' shares of the device. */
+int ss_batch_tune(ss_engine* engine, const ss_run_config* config, uint64_t first,
+                  int64_t sample, int precision, const char* cache_path);
+/* Installs the schedules recorded in a cache file written by ss_batch_tune. */
+int ss_schedule_load(const char* cache_path);
+int ss_schedule_clear(void);
+/* The schedule table as text, one "device L precision variant ns" line per
+ * entry; *needed receives the buffer size the whole text needs. */
+int ss_schedule_describe(char* buf, size_t cap, size_t* needed);
+/* Every compiled schedule: "name threads shared_bytes" per line. */
+int ss_batch_variants(char* buf, size_t cap, size_t* needed);
+
 /* -------------------------------------------------------- echo surrogate
  * No counterpart in the reference (its parameter sweeps always run the
  * exact propagator, io/Experiment.cpp:57-72).  A 6 -> 256 -> 256 -> 256 ->

@@ -582,3 +582,60 @@ def mlp_gemm_test(engine: Engine, a_bits: np.ndarray, b_bits: np.ndarray) -> np.
     check(engine.lib.ss_mlp_gemm_test(engine.handle, a.ctypes.data_as(u16), b.ctypes.data_as(u16),
                                       M, N, K, _f(c)))
     return c
+
+
+# ----------------------------------------------------------------- autotuner
+def _text(fn) -> str:
+    need = C.c_size_t()
+    check(fn(None, 0, C.byref(need)))
+    buf = C.create_string_buffer(max(need.value, 1))
+    check(fn(buf, need.value, C.byref(need)))
+    return buf.value.decode()
+
+
+def _rows(text: str):
+    out = []
+    for line in text.splitlines():
+        dev, L, prec, var, ns = line.split("\t")
+        out.append(dict(device=dev, L=int(L), precision=prec, variant=var, ns=float(ns)))
+    return out
+
+
+def variants():
+    """Every compiled batched schedule: (name, threads, shared bytes)."""
+    lib = load()
+    lib.ss_batch_variants.argtypes = [C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]
+    rows = []
+    for line in _text(lib.ss_batch_variants).splitlines():
+        name, threads, smem = line.split("\t")
+        rows.append((name, int(threads), int(smem)))
+    return rows
+
+
+def schedule():
+    """The process-wide schedule table (ss_schedule_describe)."""
+    lib = load()
+    lib.ss_schedule_describe.argtypes = [C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]
+    return _rows(_text(lib.ss_schedule_describe))
+
+
+def load_schedule(path) -> None:
+    lib = load()
+    lib.ss_schedule_load.argtypes = [C.c_char_p]
+    check(lib.ss_schedule_load(str(path).encode()))
+
+
+def clear_schedule() -> None:
+    check(load().ss_schedule_clear())
+
+
+def tune(engine: Engine, cfg: SsRunConfig, first: int = 0, sample: int = 64,
+         precision: int = abi.MIXED, cache=None):
+    """ss_batch_tune: time every candidate schedule of the config's sizes and
+    install the fastest; returns the schedule table."""
+    lib = engine.lib
+    lib.ss_batch_tune.argtypes = [C.c_void_p, C.POINTER(SsRunConfig), C.c_uint64, C.c_int64,
+                                  C.c_int, C.c_char_p]
+    check(lib.ss_batch_tune(engine.handle, C.byref(cfg), first, sample, precision,
+                            None if cache is None else str(cache).encode()))
+    return schedule()

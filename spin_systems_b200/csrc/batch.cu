@@ -8,7 +8,10 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <fstream>
 #include <map>
+#include <mutex>
+#include <sstream>
 #include <numeric>
 #include <thread>
 #include <tuple>
@@ -915,10 +918,17 @@ const std::vector<Variant>& variants() {
       make_dist_variant<14, 4, 1, float>(),     make_dist_variant<15, 4, 2, float>(),
       make_dist_variant<16, 4, 3, float>(),     make_dist_variant<13, 3, 1, double>(),
       make_dist_variant<14, 3, 2, double>(),    make_dist_variant<15, 3, 3, double>(),
+      // alternative schedules the autotuner may pick (the first entry of a
+      // size is its default): fewer register bits (more threads), or a
+      // second CTA per vector
+      make_variant<10, 3, float, PSI_SMEM>(),   make_variant<11, 3, float, PSI_SMEM>(),
+      make_variant<12, 3, float, PSI_SMEM>(),   make_dist_variant<13, 4, 1, float>(),
+      make_variant<11, 4, double, PSI_SMEM>(),  make_dist_variant<12, 3, 1, double>(),
   };
   return v;
 }
 
+// The default schedule of a size: its first entry.
 const Variant* find_variant(int L, bool mixed) {
   for (const Variant& v : variants()) {
     if (v.L == L && v.mixed == mixed) return &v;
@@ -926,7 +936,51 @@ const Variant* find_variant(int L, bool mixed) {
   return nullptr;
 }
 
+std::string variant_name(const Variant& v) {
+  static const char* homes[] = {"reg", "smem", "global"};
+  return "L" + std::to_string(v.L) + ".R" + std::to_string(v.R) + (v.mixed ? ".f32." : ".f64.") +
+         homes[v.psi] + ".c" + std::to_string(1 << v.cb);
+}
+
 }  // namespace
+
+// ------------------------------------------------------------- schedules
+// The schedule table: for (device name, L, precision) the variant the
+// autotuner measured fastest and its cost in nanoseconds per amplitude-order.
+// Batches use it for the kernel of each size bucket and, when every bucket
+// has a measured cost, for the buckets' shares of the device.  A tuning run
+// forces one candidate at a time through `g_force`.
+struct Choice {
+  std::string variant;
+  double ns = 0.0;
+};
+std::mutex g_sched_mu;
+std::map<std::tuple<std::string, int, int>, Choice> g_sched;
+thread_local const Variant* g_force = nullptr;
+
+std::string device_name(int dev) {
+  cudaDeviceProp p{};
+  SS_CUDA(cudaGetDeviceProperties(&p, dev));
+  return p.name;
+}
+
+const Variant* scheduled_variant(const std::string& dev, int L, bool mixed, double* ns) {
+  *ns = 0.0;
+  if (g_force && g_force->L == L && g_force->mixed == mixed) return g_force;
+  {
+    std::lock_guard<std::mutex> lk(g_sched_mu);
+    auto it = g_sched.find({dev, L, mixed ? 1 : 0});
+    if (it != g_sched.end()) {
+      for (const Variant& v : variants()) {
+        if (v.L == L && v.mixed == mixed && variant_name(v) == it->second.variant) {
+          *ns = it->second.ns;
+          return &v;
+        }
+      }
+    }
+  }
+  return find_variant(L, mixed);
+}
 
 // ------------------------------------------------------------------ host
 struct TypeKey {
@@ -1374,13 +1428,16 @@ void build_plan(ss_batch* b, const ss_run_config& c) {
   // share of the device in proportion to its cost, in clusters that can be
   // resident together, so that no bucket's persistent CTAs wait for another
   // bucket to drain; within a bucket the most expensive realisations go first.
-  std::vector<double> weight;
+  std::vector<double> weight, measured;
   double total_weight = 0.0;
+  const std::string dev = device_name(b->engine->device);
   for (auto& [key, list] : by_size) {
     const auto [L, mixed] = key;
     Bucket bk;
     bk.L = L;
-    bk.var = find_variant(L, mixed);
+    double ns = 0.0;
+    bk.var = scheduled_variant(dev, L, mixed, &ns);
+    measured.push_back(ns);
     if (!bk.var) {
       fail(SS_ERR_INVALID_ARGUMENT,
            std::string("the batched engine covers L = 6..") + (mixed ? "16" : "15") +
@@ -1391,10 +1448,21 @@ void build_plan(ss_batch* b, const ss_run_config& c) {
     bk.work = list;
     double w = 0.0;
     for (int x : list) w += per[x].cost;
-    w *= mixed ? 1.0 : kFp64CostFactor;
     weight.push_back(w);
-    total_weight += w;
     b->buckets.push_back(std::move(bk));
+  }
+  // Cost of a bucket: amplitude-orders times the tuned nanoseconds per
+  // amplitude-order when every bucket has been measured, else the
+  // heuristic FP64 / mixed ratio.
+  const bool all_measured =
+      std::all_of(measured.begin(), measured.end(), [](double v) { return v > 0.0; });
+  for (size_t i = 0; i < weight.size(); ++i) {
+    if (all_measured) {
+      weight[i] *= measured[i];
+    } else if (!b->buckets[i].var->mixed) {
+      weight[i] *= kFp64CostFactor;
+    }
+    total_weight += weight[i];
   }
   for (size_t i = 0; i < b->buckets.size(); ++i) {
     Bucket& bk = b->buckets[i];
@@ -1704,6 +1772,190 @@ int ss_batch_precisions(const ss_batch* b, int32_t* precision, double* amplitude
     if (precision) std::copy(b->real_precision.begin(), b->real_precision.end(), precision);
     if (amplitude_orders) {
       std::copy(b->real_amp_orders.begin(), b->real_amp_orders.end(), amplitude_orders);
+    }
+  });
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- autotuner
+namespace ss {
+namespace batch {
+namespace {
+
+void write_cache(const char* path) {
+  std::ofstream f(path, std::ios::trunc);
+  require(static_cast<bool>(f), SS_ERR_RUNTIME, "cannot write the schedule cache");
+  f << "# device\tL\tprecision\tvariant\tns_per_amplitude_order\n";
+  std::lock_guard<std::mutex> lk(g_sched_mu);
+  for (const auto& [key, ch] : g_sched) {
+    f << std::get<0>(key) << '\t' << std::get<1>(key) << '\t'
+      << (std::get<2>(key) ? "mixed" : "fp64") << '\t' << ch.variant << '\t' << ch.ns << '\n';
+  }
+}
+
+void load_cache(const char* path) {
+  std::ifstream f(path);
+  if (!f) return;  // nothing tuned yet
+  std::string line;
+  while (std::getline(f, line)) {
+    if (line.empty() || line[0] == '#') continue;
+    std::istringstream in(line);
+    std::string dev, L, prec, var, ns;
+    if (!std::getline(in, dev, '\t') || !std::getline(in, L, '\t') ||
+        !std::getline(in, prec, '\t') || !std::getline(in, var, '\t') ||
+        !std::getline(in, ns)) {
+      fail(SS_ERR_CONFIG, "malformed schedule cache line: " + line);
+    }
+    require(prec == "mixed" || prec == "fp64", SS_ERR_CONFIG, "schedule cache: unknown precision");
+    Choice c;
+    c.variant = var;
+    try {
+      c.ns = std::stod(ns);
+      const int l = std::stoi(L);
+      std::lock_guard<std::mutex> lk(g_sched_mu);
+      g_sched[{dev, l, prec == "mixed" ? 1 : 0}] = c;
+    } catch (const std::logic_error&) {
+      fail(SS_ERR_CONFIG, "malformed schedule cache line: " + line);
+    }
+  }
+}
+
+// Times one candidate on `sample` realisations of `c` (every one of size L):
+// a warm-up run, then one timed run of the captured program.
+double time_candidate(ss_engine* e, const ss_run_config& c, uint64_t first, int64_t sample,
+                      int precision, const Variant& v) {
+  ss_batch* b = nullptr;
+  g_force = &v;
+  const int rc = ss_batch_create(e, &c, first, sample, precision, &b);
+  g_force = nullptr;
+  if (rc) fail(rc, ss_last_error());
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  double ns = 0.0;
+  try {
+    if (int r = ss_batch_upload(b)) fail(r, ss_last_error());
+    if (int r = ss_batch_execute(b)) fail(r, ss_last_error());
+    SS_CUDA(cudaEventCreate(&t0));
+    SS_CUDA(cudaEventCreate(&t1));
+    SS_CUDA(cudaEventRecord(t0, e->stream));
+    if (int r = ss_batch_execute(b)) fail(r, ss_last_error());
+    SS_CUDA(cudaEventRecord(t1, e->stream));
+    SS_CUDA(cudaEventSynchronize(t1));
+    float ms = 0.0f;
+    SS_CUDA(cudaEventElapsedTime(&ms, t0, t1));
+    ns = double(ms) * 1e6 / std::max(1.0, b->amp_orders);
+  } catch (...) {
+    if (t0) cudaEventDestroy(t0);
+    if (t1) cudaEventDestroy(t1);
+    ss_batch_destroy(b);
+    throw;
+  }
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  ss_batch_destroy(b);
+  return ns;
+}
+
+}  // namespace
+}  // namespace batch
+}  // namespace ss
+
+extern "C" {
+
+int ss_batch_tune(ss_engine* e, const ss_run_config* config, uint64_t first, int64_t sample,
+                  int precision, const char* cache_path) {
+  return guarded([&] {
+    require(e != nullptr && config != nullptr, SS_ERR_INVALID_ARGUMENT, "null argument");
+    require(sample >= 1, SS_ERR_INVALID_ARGUMENT, "the tuning sample needs a realisation");
+    require(precision == SS_PRECISION_FP64 || precision == SS_PRECISION_MIXED,
+            SS_ERR_INVALID_ARGUMENT, "unknown precision");
+    if (cache_path) load_cache(cache_path);
+    const std::string dev = device_name(e->device);
+    std::vector<int> sizes;
+    if (config->n_spin_choices > 0) {
+      sizes.assign(config->spin_choices, config->spin_choices + config->n_spin_choices);
+    } else {
+      sizes.push_back(config->nspins);
+    }
+    std::sort(sizes.begin(), sizes.end());
+    sizes.erase(std::unique(sizes.begin(), sizes.end()), sizes.end());
+    std::vector<int> precs = {precision};
+    if (precision == SS_PRECISION_MIXED) precs.push_back(SS_PRECISION_FP64);  // routing target
+    for (int L : sizes) {
+      for (int prec : precs) {
+        const bool mixed = prec == SS_PRECISION_MIXED;
+        ss_run_config c = *config;
+        c.n_spin_choices = 1;  // every sampled realisation has L spins (the
+        c.spin_choices[0] = L; // per-spin tables keep the config's stride)
+        c.mixed_order_limit = -1;
+        c.sweep_points = 0;
+        c.sweep_params = nullptr;
+        Choice best;
+        for (const Variant& v : variants()) {
+          if (v.L != L || v.mixed != mixed) continue;
+          const double ns = time_candidate(e, c, first, sample, prec, v);
+          if (best.variant.empty() || ns < best.ns) {
+            best.variant = variant_name(v);
+            best.ns = ns;
+          }
+        }
+        if (best.variant.empty()) continue;  // no kernel for this size and precision
+        std::lock_guard<std::mutex> lk(g_sched_mu);
+        g_sched[{dev, L, mixed ? 1 : 0}] = best;
+      }
+    }
+    if (cache_path) write_cache(cache_path);
+  });
+}
+
+int ss_schedule_load(const char* cache_path) {
+  return guarded([&] {
+    require(cache_path != nullptr, SS_ERR_INVALID_ARGUMENT, "null path");
+    std::ifstream f(cache_path);
+    require(static_cast<bool>(f), SS_ERR_INVALID_ARGUMENT, "schedule cache not found");
+    load_cache(cache_path);
+  });
+}
+
+int ss_schedule_clear(void) {
+  return guarded([&] {
+    std::lock_guard<std::mutex> lk(g_sched_mu);
+    g_sched.clear();
+  });
+}
+
+int ss_schedule_describe(char* buf, size_t cap, size_t* needed) {
+  return guarded([&] {
+    std::ostringstream out;
+    {
+      std::lock_guard<std::mutex> lk(g_sched_mu);
+      for (const auto& [key, ch] : g_sched) {
+        out << std::get<0>(key) << '\t' << std::get<1>(key) << '\t'
+            << (std::get<2>(key) ? "mixed" : "fp64") << '\t' << ch.variant << '\t' << ch.ns << '\n';
+      }
+    }
+    const std::string text = out.str();
+    if (needed) *needed = text.size() + 1;
+    if (buf && cap > 0) {
+      const size_t n = std::min(cap - 1, text.size());
+      std::memcpy(buf, text.data(), n);
+      buf[n] = '\0';
+    }
+  });
+}
+
+int ss_batch_variants(char* buf, size_t cap, size_t* needed) {
+  return guarded([&] {
+    std::ostringstream out;
+    for (const Variant& v : variants()) {
+      out << variant_name(v) << '\t' << v.threads << '\t' << v.smem << '\n';
+    }
+    const std::string text = out.str();
+    if (needed) *needed = text.size() + 1;
+    if (buf && cap > 0) {
+      const size_t n = std::min(cap - 1, text.size());
+      std::memcpy(buf, text.data(), n);
+      buf[n] = '\0';
     }
   });
 }

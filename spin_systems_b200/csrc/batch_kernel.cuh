@@ -196,6 +196,49 @@ __device__ __forceinline__ double2 cta_sum2(double2 v, double2* red) {
   return s;
 }
 
+// The couplings (b + p, j), p < R, from one partner block: slot x of the
+// block (amplitude k ^ 2^j with register bits x) feeds the thread's slot
+// x ^ 2^p with c1[p] when that slot's bit p is set, c0[p] when it is clear.
+// MODE 1 keeps only the clear targets, MODE 2 only the set ones (the other
+// half multiplies a zero coefficient), both decided at compile time.
+template <int R, int b, int MODE, typename C2, typename Real, int NA>
+__device__ __forceinline__ void cross_apply(C2 (&acc)[NA], const C2* partner, const Real (&c0)[R],
+                                            const Real (&c1)[R]) {
+#pragma unroll
+  for (int x = 0; x < NA; ++x) {
+    const C2 v = partner[pad<R>(uint32_t(x) << b)];
+#pragma unroll
+    for (int p = 0; p < R; ++p) {
+      const int dst = x ^ (1 << p);
+      const bool set = ((dst >> p) & 1) != 0;
+      if ((MODE == 1 && set) || (MODE == 2 && !set)) continue;
+      const Real c = set ? c1[p] : c0[p];
+      acc[dst].x += c * v.x;
+      acc[dst].y += c * v.y;
+    }
+  }
+}
+
+// Without a |dd><uu| channel (has_fb false: jx == jy on every pair, as in
+// the secular dipolar couplings) a coupling (i, j) acts only on amplitudes
+// whose bits i and j differ, so when bit j is the same across the warp only
+// half of the targets receive anything: the warp takes the pruned path.
+template <int R, int b, typename C2, typename Real, int NA>
+__device__ __forceinline__ void cross_block(C2 (&acc)[NA], const C2* partner, const Real (&c0)[R],
+                                            const Real (&c1)[R], bool bj, bool has_fb) {
+  if (!has_fb) {
+    if (__all_sync(0xffffffffu, bj)) {
+      cross_apply<R, b, 1>(acc, partner, c0, c1);
+      return;
+    }
+    if (__all_sync(0xffffffffu, !bj)) {
+      cross_apply<R, b, 2>(acc, partner, c0, c1);
+      return;
+    }
+  }
+  cross_apply<R, b, 0>(acc, partner, c0, c1);
+}
+
 // One layout pass over the register group of layout g: couplings and fields
 // assigned to g are applied into acc.  For g > 0 acc is first loaded from the
 // partial buffer; own[] receives T_{n-1} of this thread's amplitudes.
@@ -289,18 +332,7 @@ __device__ __forceinline__ void layout_pass(const Smem<Real>& sm, const typename
       c1[p] = bj ? fb : ff;  // register bit set
     }
     // (kb | (x << b)) ^ m == (kb ^ m) | (x << b): bit j is not a group bit.
-    const C2* partner = cur + pad<R>(kb ^ m);
-#pragma unroll
-    for (int x = 0; x < NA; ++x) {
-      const C2 v = partner[pad<R>(uint32_t(x) << b)];
-#pragma unroll
-      for (int p = 0; p < R; ++p) {
-        const int dst = x ^ (1 << p);
-        const Real c = ((dst >> p) & 1) ? c1[p] : c0[p];
-        acc[dst].x += c * v.x;
-        acc[dst].y += c * v.y;
-      }
-    }
+    cross_block<R, b>(acc, cur + pad<R>(kb ^ m), c0, c1, bj, has_fb);
   }
 
   // Couplings (b + p, L + jb) with a CTA bit: the partner block is this
@@ -319,18 +351,7 @@ __device__ __forceinline__ void layout_pass(const Smem<Real>& sm, const typename
         c0[p] = bj ? ff : fb;
         c1[p] = bj ? fb : ff;
       }
-      const C2* partner = rcur[jb] + pad<R>(kb);
-#pragma unroll
-      for (int x = 0; x < NA; ++x) {
-        const C2 v = partner[pad<R>(uint32_t(x) << b)];
-#pragma unroll
-        for (int p = 0; p < R; ++p) {
-          const int dst = x ^ (1 << p);
-          const Real c = ((dst >> p) & 1) ? c1[p] : c0[p];
-          acc[dst].x += c * v.x;
-          acc[dst].y += c * v.y;
-        }
-      }
+      cross_block<R, b>(acc, rcur[jb] + pad<R>(kb), c0, c1, bj, has_fb);
     }
   }
 }

@@ -1,0 +1,186 @@
+"""Measurement runs for the workloads beside the headline benchmark.
+
+  uneven  4096 realisations with L drawn from {8, 10, 12, 14, 16}, sigma and
+          tau drawn from U[0.1, 1] per realisation, CPMG with 32 ideal pi_y
+          pulses: the batched mixed engine (all sizes in one graph, schedules
+          from the autotuner) against the plain FP64 path run one realisation
+          at a time (timed on a sample of each size and scaled to the batch).
+  long    Single-realisation long propagation from a random product state,
+          autonormalisation off, 10^4 steps of dt = 0.1 (sigma = 1): norm and
+          energy drift of the plain FP64 path and of the mixed engine (batch of
+          one) and the echo error of mixed against FP64.
+
+  python -m spin_systems_b200.experiments uneven [--realizations N] [--out F]
+  python -m spin_systems_b200.experiments long --nspins 16 [--steps S] [--out F]
+
+Inputs are seeded synthetic realisations (seed 20240726, streams per
+(seed, index)); device time with CUDA events on the engine's stream.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+from pathlib import Path
+
+import numpy as np
+
+from . import Batch, Engine, abi, realization_setup, run_realization, tune
+from . import workloads
+
+
+def _events(eng):
+    import torch
+    s = torch.cuda.ExternalStream(eng.stream, device=torch.device("cuda", 0))
+    return s, torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def corr0(cfg, idx, lmax):
+    out = []
+    for i in idx:
+        s = realization_setup(cfg, int(i), lmax)
+        psi = s["psi0"][0::2] + 1j * s["psi0"][1::2]
+        k = np.arange(1 << s["L"])
+        ref = sum(psi[k ^ (1 << q)] for q in range(s["L"]))
+        out.append(np.vdot(ref, ref).real)
+    return np.array(out)
+
+
+def uneven(args) -> dict:
+    eng = Engine(0)
+    spec = workloads.cpmg_uneven(realizations=args.realizations)
+    cfg = spec.config()
+    n = args.realizations
+    t0 = time.perf_counter()
+    table = tune(eng, cfg, 0, args.tune_sample, abi.MIXED)
+    tune_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    b = Batch(eng, cfg, 0, n, abi.MIXED)
+    create_s = time.perf_counter() - t0
+    stats = b.stats()
+    prec, amp = b.work()
+    sizes = np.array([realization_setup(cfg, i, 16)["L"] for i in range(n)])
+    b.upload()
+    b.execute()
+    eng.synchronize()
+    stream, e0, e1 = _events(eng)
+    e0.record(stream)
+    for _ in range(args.steps):
+        b.execute()
+    e1.record(stream)
+    e1.synchronize()
+    dev_s = e0.elapsed_time(e1) / 1e3 / args.steps
+    t0 = time.perf_counter()
+    _, mixed = b.run()
+    e2e_s = time.perf_counter() - t0
+    rep = {"workload": "uneven CPMG-32, L in {8,10,12,14,16}, sigma, tau ~ U[0.1,1]",
+           "realizations": n, "per_size": {int(L): int((sizes == L).sum()) for L in np.unique(sizes)},
+           "batched_mixed": {"seconds_per_batch": dev_s, "curves_per_s": n / dev_s,
+                             "e2e_curves_per_s": n / e2e_s,
+                             "amplitude_orders": stats["amplitude_orders"],
+                             "fp64_routed": int((prec == abi.FP64).sum()),
+                             "create_seconds": create_s},
+           "schedule": [{k: r[k] for k in ("L", "precision", "variant", "ns")} for r in table],
+           "tuning_seconds": tune_s}
+    # The FP64 reference: the plain path on a sample of each size, which also
+    # gives the echo error of those curves.
+    errs = {}
+    plain = {}
+    samples = {}
+    for L in np.unique(sizes):
+        idx = np.flatnonzero(sizes == L)[: args.plain_sample]
+        ts, es = [], []
+        scale = corr0(cfg, idx, 16)
+        for j, i in enumerate(idx):
+            t0 = time.perf_counter()
+            _, ref = run_realization(eng, cfg, int(i), b.points, b.width)
+            ts.append(time.perf_counter() - t0)
+            es.append(float(np.abs(mixed[i, :, 0] - ref[:, 0]).max() / scale[j]))
+        plain[int(L)] = float(np.mean(ts))
+        samples[int(L)] = len(idx)
+        errs[int(L)] = {"max": max(es), "mean": float(np.mean(es))}
+    plain_total = sum(plain[int(L)] * int((sizes == L).sum()) for L in np.unique(sizes))
+    rep["plain_fp64"] = {"seconds_per_realization": plain, "sampled": samples,
+                         "curves_per_s": n / plain_total,
+                         "note": "one realisation at a time through ss_run_realization, "
+                                 "timed on the sampled realisations of each size and scaled "
+                                 "by the batch's size counts"}
+    rep["speedup_batched_mixed_over_plain_fp64"] = (n / dev_s) / (n / plain_total)
+    rep["echo_error_vs_plain_fp64"] = errs
+    b._destroy()
+    eng.close()
+    return rep
+
+
+def long_run(args) -> dict:
+    eng = Engine(0)
+    L = args.nspins
+    every = args.every
+    spec = workloads.long_propagation(nspins=L, steps=args.steps, dt=0.1, every=every,
+                                      epsilon=args.epsilon)
+    cfg = spec.config()
+    points = spec.measurement_count()
+    width = spec.width()
+    rep = {"workload": f"long propagation L={L}, {args.steps} steps of dt=0.1, sigma=1, "
+                       "random product state, autonormalise off",
+           "nspins": L, "steps": args.steps, "epsilon": args.epsilon}
+    t0 = time.perf_counter()
+    times, fp64 = run_realization(eng, cfg, 0, points, width)
+    plain_s = time.perf_counter() - t0
+    # columns: norm (psi, ref), energy, corr:z (re, im)
+    norm, energy = fp64[:, 0], fp64[:, 2]
+    rep["fp64_plain"] = {"seconds": plain_s, "norm_drift": float(np.abs(norm - norm[0]).max()),
+                         "energy_drift": float(np.abs(energy - energy[0]).max()),
+                         "energy0": float(energy[0])}
+    if L <= 16:
+        b = Batch(eng, cfg, 0, 1, abi.MIXED)
+        b.upload()
+        b.execute()
+        eng.synchronize()
+        stream, e0, e1 = _events(eng)
+        e0.record(stream)
+        b.execute()
+        e1.record(stream)
+        e1.synchronize()
+        _, mixed = b.download()
+        mixed = mixed[0]
+        mnorm, menergy = mixed[:, 0], mixed[:, 2]
+        scale = abs(fp64[0, 3]) if abs(fp64[0, 3]) > 0 else 1.0
+        rep["mixed_batch_of_one"] = {
+            "seconds": e0.elapsed_time(e1) / 1e3,
+            "precision": int(b.precisions()[0]),
+            "norm_drift": float(np.abs(mnorm - mnorm[0]).max()),
+            "energy_drift": float(np.abs(menergy - menergy[0]).max()),
+            "norm_vs_fp64": float(np.abs(mnorm - norm).max()),
+            "energy_vs_fp64": float(np.abs(menergy - energy).max()),
+            "corr_z_error_vs_fp64": float(np.abs(mixed[:, 3] - fp64[:, 3]).max() / scale)}
+        b._destroy()
+    eng.close()
+    return rep
+
+
+def main(argv=None) -> None:
+    ap = argparse.ArgumentParser(description="measurement runs beside the headline benchmark")
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    u = sub.add_parser("uneven")
+    u.add_argument("--realizations", type=int, default=4096)
+    u.add_argument("--steps", type=int, default=1)
+    u.add_argument("--tune-sample", type=int, default=64)
+    u.add_argument("--plain-sample", type=int, default=2)
+    u.add_argument("--out", default="")
+    lo = sub.add_parser("long")
+    lo.add_argument("--nspins", type=int, default=16)
+    lo.add_argument("--steps", type=int, default=10000)
+    lo.add_argument("--every", type=int, default=100)
+    lo.add_argument("--epsilon", type=float, default=1e-12)
+    lo.add_argument("--out", default="")
+    args = ap.parse_args(argv)
+    rep = uneven(args) if args.cmd == "uneven" else long_run(args)
+    text = json.dumps(rep, indent=1)
+    print(text)
+    if args.out:
+        Path(args.out).write_text(text + "\n")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,12 +1,16 @@
-"""A small, self-contained case of the batched kernel for profilers.
+"""Small, self-contained cases of the engine's kernels for profilers.
 
     python -m spin_systems_b200.profile_case [--realizations N] [--blocks B]
         [--nspins L] [--precision mixed|fp64] [--repeat K]
+    python -m spin_systems_b200.profile_case --mlp [--batch B] [--steps S]
 
 Runs the XY-8 finite-pulse workload (the benchmark's shape with fewer
 realisations and XY-8 blocks) through the batched engine: one upload, then
 `repeat` executions, so a profiler can skip the first launch and capture a
-warm one.  Prints one line with the wall time per execution.
+warm one.  Prints one line with the wall time per execution.  With --mlp it
+instead trains the surrogate network for `steps` Adam steps on random data
+(batches of `batch` rows), so every tcgen05 GEMM shape of a training step
+launches `steps` times.
 """
 from __future__ import annotations
 
@@ -24,7 +28,25 @@ def main() -> None:
     ap.add_argument("--nspins", type=int, default=12)
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--repeat", type=int, default=2)
+    ap.add_argument("--mlp", action="store_true")
+    ap.add_argument("--batch", type=int, default=4096)
+    ap.add_argument("--steps", type=int, default=4)
     args = ap.parse_args()
+    if args.mlp:
+        import numpy as np
+        rng = np.random.default_rng(0)
+        x = rng.uniform(-1, 1, size=(4 * args.batch, 6)).astype(np.float32)
+        y = np.sin(x @ rng.normal(size=(6, 128))).astype(np.float32)
+        with ss.Engine(0) as eng:
+            net = ss.Mlp(eng, batch=args.batch, seed=1)
+            net.set_data(x, y)
+            t0 = time.perf_counter()
+            losses = net.train(args.steps, 1e-3, 1e-3, seed=1)
+            dt = time.perf_counter() - t0
+            print(f"profile_case mlp batch={args.batch} steps={args.steps}: "
+                  f"{dt * 1e3 / max(args.steps, 1):.3f} ms/step, loss {losses[-1]:.4g}")
+            net._destroy()
+        return
     spec = workloads.xy8_finite(nspins=args.nspins, realizations=args.realizations,
                                 blocks=args.blocks)
     prec = abi.MIXED if args.precision == "mixed" else abi.FP64
