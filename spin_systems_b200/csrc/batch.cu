@@ -1821,10 +1821,40 @@ void load_cache(const char* path) {
   }
 }
 
-// Times one candidate on `sample` realisations of `c` (every one of size L):
+// Clusters of a schedule that fit the device at once.
+int resident_clusters(const Variant& v) {
+  SS_CUDA(cudaFuncSetAttribute(v.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(v.smem)));
+  cudaLaunchConfig_t lc{};
+  cudaLaunchAttribute attr[1];
+  lc.blockDim = dim3(v.threads);
+  lc.dynamicSmemBytes = v.smem;
+  if (v.cb > 0) {
+    if (v.cluster() > 8) {
+      SS_CUDA(cudaFuncSetAttribute(v.kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    }
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = static_cast<unsigned>(v.cluster());
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    lc.attrs = attr;
+    lc.numAttrs = 1;
+    lc.gridDim = dim3(v.cluster());
+  } else {
+    lc.gridDim = dim3(2 * kClusterSize);
+  }
+  int resident = 0;
+  SS_CUDA(cudaOccupancyMaxActiveClusters(&resident, v.kernel, &lc));
+  return resident;
+}
+
+// Times one candidate on realisations of `c` (every one of size L): at least
+// `sample` and at least four waves of the candidate's resident clusters, so
+// the figure is a throughput rather than the longest realisation's latency;
 // a warm-up run, then one timed run of the captured program.
 double time_candidate(ss_engine* e, const ss_run_config& c, uint64_t first, int64_t sample,
                       int precision, const Variant& v) {
+  sample = std::max<int64_t>(sample, 4 * static_cast<int64_t>(resident_clusters(v)));
   ss_batch* b = nullptr;
   g_force = &v;
   const int rc = ss_batch_create(e, &c, first, sample, precision, &b);

@@ -239,6 +239,35 @@ __device__ __forceinline__ void cross_block(C2 (&acc)[NA], const C2* partner, co
   cross_apply<R, b, 0>(acc, partner, c0, c1);
 }
 
+// Couplings with a CTA bit from one peer block (bit uniform over the CTA, so
+// the MODE pruning of cross_apply always applies without a flip-both
+// channel): the register-bit couplings as in cross_apply, and for each of
+// the LB lowest spins (lane bits here) the partner from lane ^ 2^q.
+template <int R, int b, int MODE, int LB, typename C2, typename Real, int NA>
+__device__ __forceinline__ void cta_cross(C2 (&acc)[NA], const C2* partner, const Real (&c0)[R],
+                                          const Real (&c1)[R], const Real (&cq)[LB > 0 ? LB : 1]) {
+#pragma unroll
+  for (int x = 0; x < NA; ++x) {
+    const C2 v = partner[pad<R>(uint32_t(x) << b)];
+#pragma unroll
+    for (int p = 0; p < R; ++p) {
+      const int dst = x ^ (1 << p);
+      const bool set = ((dst >> p) & 1) != 0;
+      if ((MODE == 1 && set) || (MODE == 2 && !set)) continue;
+      const Real c = set ? c1[p] : c0[p];
+      acc[dst].x += c * v.x;
+      acc[dst].y += c * v.y;
+    }
+#pragma unroll
+    for (int q = 0; q < LB; ++q) {
+      const Real wx = __shfl_xor_sync(0xffffffffu, v.x, 1 << q);
+      const Real wy = __shfl_xor_sync(0xffffffffu, v.y, 1 << q);
+      acc[x].x += cq[q] * wx;
+      acc[x].y += cq[q] * wy;
+    }
+  }
+}
+
 // One layout pass over the register group of layout g: couplings and fields
 // assigned to g are applied into acc.  For g > 0 acc is first loaded from the
 // partial buffer; own[] receives T_{n-1} of this thread's amplitudes.
@@ -335,9 +364,16 @@ __device__ __forceinline__ void layout_pass(const Smem<Real>& sm, const typename
     cross_block<R, b>(acc, cur + pad<R>(kb ^ m), c0, c1, bj, has_fb);
   }
 
-  // Couplings (b + p, L + jb) with a CTA bit: the partner block is this
-  // thread's own block in the CTA across bit jb.
-  if constexpr (CB > 0) {
+  // Couplings (i, L + jb) with a CTA bit: the partner block is this thread's
+  // own block in the CTA across bit jb.  Layout 0 leaves its register bits'
+  // couplings to layout 1, where those spins are lane bits: there the peer
+  // block is read with consecutive lanes on consecutive amplitudes (layout
+  // 0's pattern strides 2^R + 1 elements between lanes, a separate memory
+  // sector per lane across the cluster network), and the partner of spin
+  // q < b is the same slot in lane ^ 2^q, fetched with a warp shuffle.
+  if constexpr (CB > 0 && (g > 0 || Gm::G == 1)) {
+    constexpr int LB = (g == 1 && Gm::G > 1) ? b : 0;  // layout 0's bits, here lane bits
+    static_assert(LB <= 5, "layout 0's bits must be lane bits of layout 1");
 #pragma unroll 1
     for (int jb = 0; jb < CB; ++jb) {
       const int j = L + jb;
@@ -351,7 +387,20 @@ __device__ __forceinline__ void layout_pass(const Smem<Real>& sm, const typename
         c0[p] = bj ? ff : fb;
         c1[p] = bj ? fb : ff;
       }
-      cross_block<R, b>(acc, rcur[jb] + pad<R>(kb), c0, c1, bj, has_fb);
+      Real cq[LB > 0 ? LB : 1];
+#pragma unroll
+      for (int q = 0; q < LB; ++q) {
+        const bool anti = (((t >> q) & 1u) != 0) != bj;
+        cq[q] = anti ? sm.cff[q * LS + j] : sm.cfb[q * LS + j];
+      }
+      const C2* partner = rcur[jb] + pad<R>(kb);
+      if (!has_fb && bj) {
+        cta_cross<R, b, 1, LB>(acc, partner, c0, c1, cq);
+      } else if (!has_fb) {
+        cta_cross<R, b, 2, LB>(acc, partner, c0, c1, cq);
+      } else {
+        cta_cross<R, b, 0, LB>(acc, partner, c0, c1, cq);
+      }
     }
   }
 }
