@@ -12,6 +12,7 @@
 
   python -m spin_systems_b200.experiments uneven [--realizations N] [--out F]
   python -m spin_systems_b200.experiments long --nspins 16 [--steps S] [--out F]
+  python -m spin_systems_b200.experiments plain [--sizes 16 20 22 24] [--out F]
 
 Inputs are seeded synthetic realisations (seed 20240726, streams per
 (seed, index)); device time with CUDA events on the engine's stream.
@@ -61,7 +62,8 @@ def uneven(args) -> dict:
     prec, amp = b.work()
     sizes = np.array([realization_setup(cfg, i, 16)["L"] for i in range(n)])
     b.upload()
-    b.execute()
+    for _ in range(args.warmup):
+        b.execute()
     eng.synchronize()
     stream, e0, e1 = _events(eng)
     e0.record(stream)
@@ -159,12 +161,69 @@ def long_run(args) -> dict:
     return rep
 
 
+
+def plain(args) -> dict:
+    """The plain FP64 path's kernels on single large vectors: the fused
+    Chebyshev-order kernel at each L (effective bandwidth at the algorithmic
+    80 B per amplitude-order, and anti-aligned pair terms applied per
+    second), and the streaming StateVector kernels at L = 26 (1 GiB vectors),
+    which have no partner gathers."""
+    from . import Hamiltonian, Propagator, StateVector
+    eng = Engine(0)
+    stream, e0, e1 = _events(eng)
+    rep = {"order_kernel": {}, "streaming": {}}
+    for L in args.sizes:
+        spec = workloads.long_propagation(nspins=L, steps=1, every=1, epsilon=1e-7)
+        cfg = spec.config()
+        s = realization_setup(cfg, 0, L)
+        ham = Hamiltonian(eng, L, s["fields"], s["pairs"], s["J"])
+        psi = StateVector(eng, L, s["psi0"])
+        prop = Propagator(L, 1e-7)
+        prop.evolve(ham, abi.REAL, psi, 0.1, 1)          # warm-up, builds the tables
+        eng.synchronize()
+        e0.record(stream)
+        prop.evolve(ham, abi.REAL, psi, 0.1, args.steps)
+        e1.record(stream)
+        e1.synchronize()
+        sec = e0.elapsed_time(e1) / 1e3
+        orders = prop.last_order * args.steps
+        amps = float(1 << L)
+        npairs = len(s["pairs"]) // 2
+        rep["order_kernel"][int(L)] = {
+            "orders": int(orders), "ms_per_order": 1e3 * sec / orders,
+            "effective_gbs_at_80B": 80.0 * amps * orders / sec / 1e9,
+            "pair_terms_per_s": 0.5 * npairs * amps * orders / sec, "pairs": npairs}
+        del psi, ham
+    L = 26
+    a = StateVector(eng, L)
+    b = StateVector(eng, L)
+    a.set_basis_state(0)
+    b.set_basis_state(1)
+    n = float(1 << L)
+    for name, fn, nbytes in (("add_scaled", lambda: a.add_scaled(0.5, 0.25, b), 48.0),
+                             ("scale", lambda: a.scale(1.0), 32.0),
+                             ("norm", lambda: a.norm(), 16.0)):
+        fn()
+        eng.synchronize()
+        reps = 20
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+        sec = e0.elapsed_time(e1) / 1e3 / reps
+        rep["streaming"][name] = {"bytes_per_amp": nbytes, "gbs": nbytes * n / sec / 1e9}
+    eng.close()
+    return rep
+
 def main(argv=None) -> None:
     ap = argparse.ArgumentParser(description="measurement runs beside the headline benchmark")
     sub = ap.add_subparsers(dest="cmd", required=True)
     u = sub.add_parser("uneven")
     u.add_argument("--realizations", type=int, default=4096)
     u.add_argument("--steps", type=int, default=1)
+    u.add_argument("--warmup", type=int, default=0,
+                   help="untimed runs first (the graph is instantiated at creation)")
     u.add_argument("--tune-sample", type=int, default=64)
     u.add_argument("--plain-sample", type=int, default=2)
     u.add_argument("--out", default="")
@@ -174,8 +233,12 @@ def main(argv=None) -> None:
     lo.add_argument("--every", type=int, default=100)
     lo.add_argument("--epsilon", type=float, default=1e-12)
     lo.add_argument("--out", default="")
+    pl = sub.add_parser("plain")
+    pl.add_argument("--sizes", type=int, nargs="+", default=[16, 20, 22, 24])
+    pl.add_argument("--steps", type=int, default=2)
+    pl.add_argument("--out", default="")
     args = ap.parse_args(argv)
-    rep = uneven(args) if args.cmd == "uneven" else long_run(args)
+    rep = {"uneven": uneven, "long": long_run, "plain": plain}[args.cmd](args)
     text = json.dumps(rep, indent=1)
     print(text)
     if args.out:
