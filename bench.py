@@ -8,6 +8,10 @@ correlator at 128 times, state and reference propagated together.  Inputs are
 seeded synthetic realisations (seed 20240726, streams per (seed, index)).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+  python bench.py --workload cpmg10      the reference's own CPU-runnable case:
+      L = 10 ideal-pulse CPMG (pi/2_x, then 8 x (0.5, pi_y, 0.5, measure)),
+      sigma = 0.5, 20 realisations, complex128 -- batched FP64 and mixed,
+      the plain FP64 path and the reference's CPU build on the same 20
 
 One JSON line on stdout from rank 0.  Multi-GPU: one process per GPU (torchrun),
 each rank runs its own 1024 realisations (disjoint index ranges, no device
@@ -334,6 +338,67 @@ def run_ours(args):
     eng.close()
 
 
+
+def run_cpmg10(args):
+    """The L = 10 CPMG of the reference's demo config: every path on the same
+    20 realisations, device time with CUDA events, the reference's CPU build
+    on all host threads (wall clock around its experiment)."""
+    import torch
+    import spin_systems_b200 as ss
+    from spin_systems_b200 import abi, workloads
+    from oracle.oracle import Port, Ref
+    spec = workloads.cpmg_ideal()
+    cfg = spec.config()
+    n = spec.realizations
+    eng = ss.Engine(0)
+    stream = torch.cuda.ExternalStream(eng.stream, device=torch.device("cuda", 0))
+    out = {}
+    for name, prec in (("batched_fp64", abi.FP64), ("batched_mixed", abi.MIXED)):
+        b = ss.Batch(eng, cfg, 0, n, prec)
+        b.upload()
+        for _ in range(max(args.warmup, 3)):
+            b.execute()
+        eng.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            b.execute()
+        e1.record(stream)
+        e1.synchronize()
+        sec = e0.elapsed_time(e1) / 1e3 / args.steps
+        t0 = time.perf_counter()
+        _, rows = b.run()
+        e2e = time.perf_counter() - t0
+        out[name] = {"curves_per_s": n / sec, "e2e_curves_per_s": n / e2e, "rows": rows}
+        del b
+    ss.run_realization(eng, cfg, 0, spec.measurement_count(), spec.width())
+    t0 = time.perf_counter()
+    plain = [ss.run_realization(eng, cfg, i, spec.measurement_count(), spec.width())[1]
+             for i in range(n)]
+    out["plain_fp64"] = {"curves_per_s": n / (time.perf_counter() - t0)}
+    threads = cpu_threads()
+    lib, kind = (Ref(), "reference") if Ref.available() else (Port(), "port")
+    _, want, secs = lib.run_range(cfg, 0, n, threads)
+    want = np.asarray(want).reshape(out["batched_fp64"]["rows"].shape)
+    scale = np.abs(want[:, :, 0]).max()
+    line = {"metric": "echo curves/s, L=10 CPMG (20 realisations)", "unit": UNIT,
+            "value": out["batched_fp64"]["curves_per_s"], "n_gpus": 1, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "higher_is_better": True, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": "L=10 CPMG pi/2_x + 8x(0.5, pi_y, 0.5), "
+                                             "sigma=0.5, 20 realisations, corr:x + norm"},
+            "batched_fp64": {k: v for k, v in out["batched_fp64"].items() if k != "rows"},
+            "batched_mixed": {k: v for k, v in out["batched_mixed"].items() if k != "rows"},
+            "plain_fp64": out["plain_fp64"],
+            "parity_vs_cpu_reference": {
+                "batched_fp64_max_abs": float(np.abs(out["batched_fp64"]["rows"] - want).max()),
+                "plain_fp64_max_abs": float(np.abs(np.stack(plain) - want).max()),
+                "batched_mixed_echo_error": float(np.abs(out["batched_mixed"]["rows"][:, :, 0]
+                                                         - want[:, :, 0]).max() / scale)},
+            "cpu_baseline": {"value": n / secs, "unit": UNIT, "cores": threads, "kind": kind,
+                             "sample": f"all {n} realisations on {threads} threads"}}
+    print(json.dumps(line), flush=True)
+    eng.close()
+
 _SMS = [148]
 
 
@@ -355,8 +420,12 @@ def main():
                     help="run the autotuner before timing (default)")
     ap.add_argument("--no-tune", dest="tune", action="store_false")
     ap.add_argument("--tune-sample", type=int, default=296)
+    ap.add_argument("--workload", choices=["xy8", "cpmg10"], default="xy8",
+                    help="xy8: the headline batch (default); cpmg10: the L=10 demo case")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.workload == "cpmg10" and args.impl == "ours":
+        run_cpmg10(args)
+    elif args.impl == "reference":
         run_reference_arm(args)
     else:
         run_ours(args)

@@ -924,6 +924,10 @@ const std::vector<Variant>& variants() {
       make_variant<10, 3, float, PSI_SMEM>(),   make_variant<11, 3, float, PSI_SMEM>(),
       make_variant<12, 3, float, PSI_SMEM>(),   make_dist_variant<13, 4, 1, float>(),
       make_variant<11, 4, double, PSI_SMEM>(),  make_dist_variant<12, 3, 1, double>(),
+      // cluster sizes with five register bits: 256 threads of 32 amplitudes,
+      // three layouts instead of four and no 128-register cap
+      make_dist_variant<14, 5, 1, float>(),     make_dist_variant<15, 5, 2, float>(),
+      make_dist_variant<16, 5, 3, float>(),
   };
   return v;
 }

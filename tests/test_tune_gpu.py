@@ -14,7 +14,7 @@ pytestmark = pytest.mark.gpu
 def _spec():
     spec = workloads.cpmg_uneven(realizations=8, pulses=2)
     spec.spin_choices = (10, 11, 12, 13)
-    spec.nspins = 13
+    spec.nspins = 16
     spec.tau_range = (0.05, 0.2)
     return spec
 
@@ -35,7 +35,9 @@ def test_tuner_fills_the_table_and_writes_the_cache(engine, tmp_path):
 
 @pytest.mark.parametrize("variant", ["L10.R3.f32.smem.c1", "L11.R3.f32.smem.c1",
                                      "L12.R3.f32.smem.c1", "L13.R4.f32.global.c2",
-                                     "L11.R4.f64.smem.c1", "L12.R3.f64.global.c2"])
+                                     "L11.R4.f64.smem.c1", "L12.R3.f64.global.c2",
+                                     "L14.R5.f32.global.c2", "L15.R5.f32.global.c4",
+                                     "L16.R5.f32.global.c8"])
 def test_every_alternative_schedule_matches_the_oracle(engine, port, tmp_path, variant):
     ss.clear_schedule()
     spec = _spec()
@@ -57,7 +59,7 @@ def test_every_alternative_schedule_matches_the_oracle(engine, port, tmp_path, v
     else:
         scale = []
         for i in range(3):
-            s = ss.realization_setup(cfg, i, 13)
+            s = ss.realization_setup(cfg, i, 16)
             psi = s["psi0"][0::2] + 1j * s["psi0"][1::2]
             k = np.arange(1 << s["L"])
             ref = sum(psi[k ^ (1 << q)] for q in range(s["L"]))
