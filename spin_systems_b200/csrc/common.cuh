@@ -39,6 +39,24 @@ constexpr int kMaxReduceBlocks = 1184;      // 8 x 148 SMs
 
 }  // namespace ss
 
+namespace ss {
+// One captured Chebyshev step of the plain propagator (init + every order +
+// the optional renormalisation) for fixed vectors, tables and weights.
+struct StepGraph {
+  const void* terms = nullptr;
+  const void* diag = nullptr;
+  const void* psi = nullptr;
+  const void* t0 = nullptr;
+  const void* t1 = nullptr;
+  size_t n = 0;
+  int autonormalize = 0;
+  std::vector<double> weights;
+  cudaGraphExec_t exec = nullptr;
+  int64_t kernels = 0;  // kernel nodes per replay
+  uint64_t used = 0;    // last use, for eviction
+};
+}  // namespace ss
+
 // Device-side scratch of one engine: reduction partials, the completion
 // counter of the last-block reduction and result slots read by the host.
 struct ss_engine {
@@ -53,6 +71,8 @@ struct ss_engine {
   int* host_flags = nullptr;
   double2* evolve_t[2] = {nullptr, nullptr};  // the propagator's two work vectors
   int evolve_nspins = 0;                      // their capacity, as L
+  std::vector<ss::StepGraph> step_graphs;     // the plain propagator's captured steps
+  uint64_t graph_clock = 0;
   std::atomic<int64_t> launches{0};
 };
 

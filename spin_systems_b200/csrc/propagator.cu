@@ -3,6 +3,7 @@
 // amplitude and its partners), T_{n-2} and psi, and writes T_n over T_{n-2}
 // and psi += c_n T_n -- the recurrence, the Hamiltonian and the series update
 // in a single pass instead of the reference's 1 + L + P + 3 passes.
+#include <algorithm>
 #include <cmath>
 
 #include "hamiltonian.cuh"
@@ -81,7 +82,8 @@ void evolve_fp64(ss_ham* h, ss_state* psi, const std::vector<double>& weights, d
   ensure_evolve_scratch(e, h->nspins);
   const size_t n = h->size();
   const unsigned int grid = blocks_for(n);
-  for (int64_t step = 0; step < nsteps; ++step) {
+  // One step: T_0, every order, the optional renormalisation.
+  auto one_step = [&] {
     double2* cur = e->evolve_t[0];
     double2* prev = e->evolve_t[1];
     launch(e, k_cheb_init, grid, kThreads, 0, psi->data, cur, n, weights[0]);
@@ -91,6 +93,62 @@ void evolve_fp64(ss_ham* h, ss_state* psi, const std::vector<double>& weights, d
       std::swap(cur, prev);
     }
     if (autonormalize) state_normalize_async(psi, 1);
+  };
+  // The step is captured once as a CUDA graph per (vectors, tables,
+  // weights) and replayed: a pulse program repeats a handful of expansions on
+  // the same two vectors, and one graph launch replaces ncoef kernel launches
+  // (the launch rate, not the GPU, bounds small L).  The replay issues the
+  // same kernels with the same arguments in the same order.
+  StepGraph* g = nullptr;
+  for (StepGraph& c : e->step_graphs) {
+    if (c.terms == h->dev_terms && c.diag == h->diag && c.psi == psi->data &&
+        c.t0 == e->evolve_t[0] && c.t1 == e->evolve_t[1] && c.n == n &&
+        c.autonormalize == int(autonormalize) && c.weights == weights) {
+      g = &c;
+      break;
+    }
+  }
+  if (g == nullptr) {
+    constexpr size_t kMaxGraphs = 32;
+    if (e->step_graphs.size() >= kMaxGraphs) {
+      auto old = std::min_element(e->step_graphs.begin(), e->step_graphs.end(),
+                                  [](const StepGraph& a, const StepGraph& b) { return a.used < b.used; });
+      if (old->exec) cudaGraphExecDestroy(old->exec);
+      e->step_graphs.erase(old);
+    }
+    StepGraph c;
+    c.terms = h->dev_terms;
+    c.diag = h->diag;
+    c.psi = psi->data;
+    c.t0 = e->evolve_t[0];
+    c.t1 = e->evolve_t[1];
+    c.n = n;
+    c.autonormalize = int(autonormalize);
+    c.weights = weights;
+    const int64_t before = e->launches.load();
+    cudaGraph_t graph = nullptr;
+    SS_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+    try {
+      one_step();
+    } catch (...) {
+      cudaStreamEndCapture(e->stream, &graph);
+      if (graph) cudaGraphDestroy(graph);
+      e->launches.store(before);
+      throw;
+    }
+    SS_CUDA(cudaStreamEndCapture(e->stream, &graph));
+    const cudaError_t ie = cudaGraphInstantiate(&c.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    SS_CUDA(ie);
+    c.kernels = e->launches.load() - before;
+    e->launches.store(before);
+    e->step_graphs.push_back(std::move(c));
+    g = &e->step_graphs.back();
+  }
+  g->used = ++e->graph_clock;
+  for (int64_t step = 0; step < nsteps; ++step) {
+    SS_CUDA(cudaGraphLaunch(g->exec, e->stream));
+    e->launches.fetch_add(g->kernels, std::memory_order_relaxed);
   }
   if (autonormalize) check_flags(e);
 }

@@ -201,6 +201,9 @@ int ss_engine_destroy(ss_engine* e) {
     cudaFree(e->dev_flags);
     cudaFree(e->evolve_t[0]);
     cudaFree(e->evolve_t[1]);
+    for (ss::StepGraph& g : e->step_graphs) {
+      if (g.exec) cudaGraphExecDestroy(g.exec);
+    }
     cudaFreeHost(e->host_result);
     cudaFreeHost(e->host_flags);
     if (e->stream) cudaStreamDestroy(e->stream);

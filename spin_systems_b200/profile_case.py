@@ -28,6 +28,8 @@ def main() -> None:
     ap.add_argument("--nspins", type=int, default=12)
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--repeat", type=int, default=2)
+    ap.add_argument("--variant", default="",
+                    help="force this schedule for the size (see spin_systems_b200.variants())")
     ap.add_argument("--mlp", action="store_true")
     ap.add_argument("--batch", type=int, default=4096)
     ap.add_argument("--steps", type=int, default=4)
@@ -50,6 +52,13 @@ def main() -> None:
     spec = workloads.xy8_finite(nspins=args.nspins, realizations=args.realizations,
                                 blocks=args.blocks)
     prec = abi.MIXED if args.precision == "mixed" else abi.FP64
+    if args.variant:
+        import tempfile
+        import torch
+        dev = torch.cuda.get_device_name(0)
+        with tempfile.NamedTemporaryFile("w", suffix=".tsv", delete=False) as f:
+            f.write(f"{dev}\t{args.nspins}\t{args.precision}\t{args.variant}\t1.0\n")
+        ss.load_schedule(f.name)
     with ss.Engine(0) as eng:
         batch = ss.Batch(eng, spec.config(), 0, args.realizations, prec)
         batch.upload()
@@ -60,7 +69,7 @@ def main() -> None:
             dt = time.perf_counter() - t0
         stats = batch.stats()
         print(f"profile_case L={args.nspins} n={args.realizations} blocks={args.blocks} "
-              f"{args.precision}: {dt * 1e3:.2f} ms/execute, "
+              f"{args.precision} {args.variant or 'default'}: {dt * 1e3:.2f} ms/execute, "
               f"{stats['amplitude_orders']:.3e} amplitude-orders")
         del batch
 
