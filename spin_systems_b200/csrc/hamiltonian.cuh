@@ -55,6 +55,9 @@ __device__ __forceinline__ double2 ham_gather(const HamTerms* __restrict__ t,
     re += cx * p.x - cy * p.y;
     im += cx * p.y + cy * p.x;
   }
+  // Unrolled so that several partner loads are in flight per thread: the
+  // loop is bound by their latency, not by the two FMAs each feeds.
+#pragma unroll 8
   for (int i = 0; i < t->npair; ++i) {
     const unsigned int lo = t->pair_lo[i], hi = t->pair_hi[i];
     const bool aligned = ((k & lo) != 0) == ((k & hi) != 0);
