@@ -202,6 +202,15 @@ def run_reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+
+def kernel_desc(tuned):
+    """The schedules the timed graph ran: the tuner's choice, else the defaults."""
+    chosen = {r["precision"]: r["variant"] for r in tuned if r["L"] == L}
+    mixed = chosen.get("mixed", "L12.R4.f32.smem.c1")
+    fp64 = chosen.get("fp64", "L12.R3.f64.global.c1")
+    return (f"{mixed} (mixed bucket) with the routed realisations in {fp64} (FP64 bucket) of "
+            "the same graph; the recursion is resident in shared memory")
+
 def run_ours(args):
     import torch
     rank, world, local = dist_setup(args.gpus)
@@ -306,9 +315,7 @@ def run_ours(args):
                      "traffic_note": "DRAM bytes of the mixed kernel per launch, scaled from "
                                      "an ncu capture of a smaller case by amplitude-orders",
                      "peak_source": src,
-                     "kernel": "k_batch<12,4,float> with the routed realisations in "
-                               "k_batch<12,3,double> of the same graph (state vectors resident "
-                               "in shared memory)",
+                     "kernel": kernel_desc(tuned),
                      "algorithmic_bytes_per_launch": alg_bytes,
                      "note": "effective bandwidth of a shared-memory-resident kernel pair; the "
                              "binding limit is shared-memory bandwidth and issue (see smem)"},

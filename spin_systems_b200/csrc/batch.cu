@@ -928,6 +928,10 @@ const std::vector<Variant>& variants() {
       // three layouts instead of four and no 128-register cap
       make_dist_variant<14, 5, 1, float>(),     make_dist_variant<15, 5, 2, float>(),
       make_dist_variant<16, 5, 3, float>(),
+      // L = 12 with four register bits in FP64 (256 threads of 16
+      // amplitudes) and with the FP32 path's psi in registers; both keep one
+      // CTA per SM, which the buckets' shares of the device assume
+      make_variant<12, 4, double, PSI_GLOBAL>(), make_variant<12, 4, float, PSI_REG>(),
   };
   return v;
 }

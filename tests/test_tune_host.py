@@ -13,7 +13,7 @@ def test_every_size_has_a_default_and_the_alternatives_are_listed():
     assert sizes_mixed == set(range(6, 17)) and sizes_fp64 == set(range(6, 16))
     # sizes with a choice to make
     for L in (10, 11, 12, 13, 14, 15, 16):
-        assert sum(n.startswith(f"L{L}.") and ".f32." in n for n in names) == 2
+        assert sum(n.startswith(f"L{L}.") and ".f32." in n for n in names) >= 2
     assert "L16.R4.f32.global.c8" in names
     for name, threads, smem in ss.variants():
         assert 32 <= threads <= 1024 and smem <= 232448
