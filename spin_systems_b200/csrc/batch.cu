@@ -1451,6 +1451,10 @@ void build_plan(ss_batch* b, const ss_run_config& c) {
            std::string("the batched engine covers L = 6..") + (mixed ? "16" : "15") +
                " in this precision; got L = " + std::to_string(L));
     }
+    // The cluster kernel's measurement keeps one partial sum per observable
+    // in a fixed shared slot array.
+    require(bk.var->cb == 0 || b->obs.size() / 3 <= static_cast<size_t>(kMaxDistObs),
+            SS_ERR_CONFIG, "sizes above 13 spins (FP32) / 12 (FP64) measure at most 8 observables");
     std::stable_sort(list.begin(), list.end(),
                      [&](int x, int y) { return per[x].cost > per[y].cost; });
     bk.work = list;

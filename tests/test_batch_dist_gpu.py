@@ -92,3 +92,14 @@ def test_uneven_batch_up_to_l16_in_one_launch(engine, port):
     for i in range(10):
         err = np.abs(rows[i, :, 0] - want[i][:, 0]).max() / scale[i]
         assert err < ECHO_TOL, (i, Ls[i], err)
+
+
+def test_cluster_sizes_cap_the_observable_count(engine):
+    # The cluster kernel's measurement holds at most eight observables; the
+    # batch refuses more when it is built, before any launch.
+    spec = short_spec(14, 1)
+    spec.observables = ["corr:x", "corr:y", "corr:z", "norm", "energy"] + \
+        [f"mag:{s}:x" for s in range(1, 6)]
+    with pytest.raises(ss.SpinsimError) as e:
+        ss.Batch(engine, spec.config(), 0, 1, abi.MIXED)
+    assert e.value.kind == "config"

@@ -107,3 +107,4 @@ def test_program_flattening_counts_measurements():
     cfg = spec.config()
     assert cfg.n_steps == 1 + 8 * 4
     assert cfg.steps[0].kind == abi.REPEAT and cfg.steps[0].body_len == 32
+
