@@ -932,6 +932,10 @@ const std::vector<Variant>& variants() {
       // amplitudes) and with the FP32 path's psi in registers; both keep one
       // CTA per SM, which the buckets' shares of the device assume
       make_variant<12, 4, double, PSI_GLOBAL>(), make_variant<12, 4, float, PSI_REG>(),
+      // psi in registers for the FP64 routing target at L = 12 and the
+      // mid-size FP32 schedules
+      make_variant<12, 3, double, PSI_REG>(),   make_variant<12, 4, double, PSI_REG>(),
+      make_variant<11, 4, float, PSI_REG>(),    make_variant<10, 4, float, PSI_REG>(),
   };
   return v;
 }

@@ -119,18 +119,43 @@ def exact(engine: Engine, p: np.ndarray, realizations: int, precision: int = abi
     return out
 
 
+def _groups(p: np.ndarray):
+    """Indices of each (sequence, L) group."""
+    key = p["sequence"].astype(np.int64) * 64 + p["nspins"].astype(np.int64)
+    for k in np.unique(key):
+        yield k, np.flatnonzero(key == k)
+
+
+def _nearest(ref_x: np.ndarray, q_x: np.ndarray, k: int, chunk: int = 4096) -> np.ndarray:
+    """Indices of the k nearest rows of ref_x for every row of q_x (squared
+    Euclidean distance on the continuous features), in chunks of queries."""
+    out = np.zeros((len(q_x), k), dtype=np.int64)
+    rn = (ref_x ** 2).sum(axis=1)
+    for at in range(0, len(q_x), chunk):
+        q = q_x[at:at + chunk]
+        d = (q ** 2).sum(axis=1)[:, None] + rn[None, :] - 2.0 * q @ ref_x.T
+        if k >= ref_x.shape[0]:
+            idx = np.argsort(d, axis=1)[:, :k]
+        else:
+            idx = np.argpartition(d, k - 1, axis=1)[:, :k]
+        out[at:at + chunk, :idx.shape[1]] = idx
+        if idx.shape[1] < k:
+            out[at:at + chunk, idx.shape[1]:] = idx[:, -1:]
+    return out
+
+
 def nearest_neighbour(train_p: np.ndarray, train_y: np.ndarray, query: np.ndarray) -> np.ndarray:
     """The method without a network: the closest precomputed curve (feature
-    distance, same sequence and L)."""
-    fx, fq = features(train_p), features(query)
+    distance, same sequence and L; any curve if the group has none)."""
+    fx, fq = features(train_p).astype(np.float64), features(query).astype(np.float64)
     out = np.zeros((len(query), POINTS))
-    for i in range(len(query)):
-        same = (train_p["sequence"] == query["sequence"][i]) & (train_p["nspins"] == query["nspins"][i])
-        cand = np.flatnonzero(same)
+    tkey = train_p["sequence"].astype(np.int64) * 64 + train_p["nspins"].astype(np.int64)
+    for key, qi in _groups(query):
+        cand = np.flatnonzero(tkey == key)
         if len(cand) == 0:
             cand = np.arange(len(train_p))
-        d = ((fx[cand, :4] - fq[i, :4]) ** 2).sum(axis=1)
-        out[i] = train_y[cand[int(np.argmin(d))]]
+        near = _nearest(fx[cand, :4], fq[qi, :4], 1)[:, 0]
+        out[qi] = train_y[cand[near]]
     return out
 
 
@@ -163,15 +188,15 @@ class Surrogate:
         est = np.full(len(p), np.inf)
         if self.cal_x is None:
             return est
-        fq = features(p)
-        for i in range(len(p)):
-            same = np.flatnonzero((self.cal_p["sequence"] == p["sequence"][i]) &
-                                  (self.cal_p["nspins"] == p["nspins"][i]))
+        fq = features(p).astype(np.float64)
+        cx = self.cal_x.astype(np.float64)
+        ckey = self.cal_p["sequence"].astype(np.int64) * 64 + self.cal_p["nspins"].astype(np.int64)
+        for key, qi in _groups(p):
+            same = np.flatnonzero(ckey == key)
             if len(same) == 0:
                 continue
-            d = ((self.cal_x[same, :4] - fq[i, :4]) ** 2).sum(axis=1)
-            near = same[np.argsort(d)[:k]]
-            est[i] = safety * self.cal_err[near].max()
+            near = _nearest(cx[same, :4], fq[qi, :4], min(k, len(same)))
+            est[qi] = safety * self.cal_err[same[near]].max(axis=1)
         return est
 
     def predict(self, p: np.ndarray, fallback: Callable[[np.ndarray], np.ndarray],
