@@ -360,6 +360,9 @@ def run_cpmg10(args):
     eng = ss.Engine(0)
     stream = torch.cuda.ExternalStream(eng.stream, device=torch.device("cuda", 0))
     out = {}
+    tuned = []
+    if args.tune:  # schedules for L = 10 in both precisions (mixed run includes FP64)
+        tuned = ss.tune(eng, cfg, 0, n, abi.MIXED)
     for name, prec in (("batched_fp64", abi.FP64), ("batched_mixed", abi.MIXED)):
         b = ss.Batch(eng, cfg, 0, n, prec)
         b.upload()
@@ -402,7 +405,8 @@ def run_cpmg10(args):
                 "batched_mixed_echo_error": float(np.abs(out["batched_mixed"]["rows"][:, :, 0]
                                                          - want[:, :, 0]).max() / scale)},
             "cpu_baseline": {"value": n / secs, "unit": UNIT, "cores": threads, "kind": kind,
-                             "sample": f"all {n} realisations on {threads} threads"}}
+                             "sample": f"all {n} realisations on {threads} threads"},
+            "schedule": [{k: r[k] for k in ("L", "precision", "variant", "ns")} for r in tuned]}
     print(json.dumps(line), flush=True)
     eng.close()
 

@@ -936,6 +936,7 @@ const std::vector<Variant>& variants() {
       // mid-size FP32 schedules
       make_variant<12, 3, double, PSI_REG>(),   make_variant<12, 4, double, PSI_REG>(),
       make_variant<11, 4, float, PSI_REG>(),    make_variant<10, 4, float, PSI_REG>(),
+      make_variant<10, 3, double, PSI_REG>(),   make_variant<11, 3, double, PSI_REG>(),
   };
   return v;
 }

@@ -40,7 +40,8 @@ def test_tuner_fills_the_table_and_writes_the_cache(engine, tmp_path):
                                      "L16.R5.f32.global.c8", "L12.R4.f64.global.c1",
                                      "L12.R4.f32.reg.c1", "L12.R3.f64.reg.c1",
                                      "L12.R4.f64.reg.c1", "L11.R4.f32.reg.c1",
-                                     "L10.R4.f32.reg.c1"])
+                                     "L10.R4.f32.reg.c1", "L10.R3.f64.reg.c1",
+                                     "L11.R3.f64.reg.c1"])
 def test_every_alternative_schedule_matches_the_oracle(engine, port, tmp_path, variant):
     ss.clear_schedule()
     spec = _spec()
