@@ -13,6 +13,7 @@
   python -m spin_systems_b200.experiments uneven [--realizations N] [--out F]
   python -m spin_systems_b200.experiments long --nspins 16 [--steps S] [--out F]
   python -m spin_systems_b200.experiments plain [--sizes 16 20 22 24] [--out F]
+  python -m spin_systems_b200.experiments per_size [--sizes 12 14 16] [--out F]
 
 Inputs are seeded synthetic realisations (seed 20240726, streams per
 (seed, index)); device time with CUDA events on the engine's stream.
@@ -89,8 +90,10 @@ def uneven(args) -> dict:
     errs = {}
     plain = {}
     samples = {}
+    plain_total = 0.0
     for L in np.unique(sizes):
-        idx = np.flatnonzero(sizes == L)[: args.plain_sample]
+        members = np.flatnonzero(sizes == L)
+        idx = members[: args.plain_sample]
         ts, es = [], []
         scale = corr0(cfg, idx, 16)
         for j, i in enumerate(idx):
@@ -98,15 +101,17 @@ def uneven(args) -> dict:
             _, ref = run_realization(eng, cfg, int(i), b.points, b.width)
             ts.append(time.perf_counter() - t0)
             es.append(float(np.abs(mixed[i, :, 0] - ref[:, 0]).max() / scale[j]))
-        plain[int(L)] = float(np.mean(ts))
+        # seconds per amplitude-order of the sample, times the size's work
+        size_s = sum(ts) * float(amp[members].sum()) / float(amp[idx].sum())
+        plain_total += size_s
+        plain[int(L)] = size_s / len(members)
         samples[int(L)] = len(idx)
         errs[int(L)] = {"max": max(es), "mean": float(np.mean(es))}
-    plain_total = sum(plain[int(L)] * int((sizes == L).sum()) for L in np.unique(sizes))
     rep["plain_fp64"] = {"seconds_per_realization": plain, "sampled": samples,
                          "curves_per_s": n / plain_total,
                          "note": "one realisation at a time through ss_run_realization, "
                                  "timed on the sampled realisations of each size and scaled "
-                                 "by the batch's size counts"}
+                                 "by that size's amplitude-orders in the batch"}
     rep["speedup_batched_mixed_over_plain_fp64"] = (n / dev_s) / (n / plain_total)
     rep["echo_error_vs_plain_fp64"] = errs
     b._destroy()
@@ -216,6 +221,53 @@ def plain(args) -> dict:
     eng.close()
     return rep
 
+
+def per_size(args) -> dict:
+    """The uneven batch's program (CPMG-32, sigma and tau ~ U[0.1, 1]) at one
+    L at a time: the batched mixed engine (tuned) on enough realisations to
+    fill the device, against the plain FP64 path on a sample of the same
+    realisations, one at a time."""
+    eng = Engine(0)
+    rep = {}
+    for L, n in zip(args.sizes, args.counts):
+        spec = workloads.cpmg_uneven(realizations=n)
+        spec.spin_choices = (L,)
+        cfg = spec.config()
+        tune(eng, cfg, 0, min(n, 64), abi.MIXED)
+        b = Batch(eng, cfg, 0, n, abi.MIXED)
+        b.upload()
+        b.execute()
+        eng.synchronize()
+        stream, e0, e1 = _events(eng)
+        e0.record(stream)
+        b.execute()
+        e1.record(stream)
+        e1.synchronize()
+        sec = e0.elapsed_time(e1) / 1e3
+        _, mixed = b.download()
+        _, amp = b.work()
+        ts, es = [], []
+        scale = corr0(cfg, range(args.plain_sample), 16)
+        for i in range(args.plain_sample):
+            t0 = time.perf_counter()
+            _, ref = run_realization(eng, cfg, i, b.points, b.width)
+            ts.append(time.perf_counter() - t0)
+            es.append(float(np.abs(mixed[i, :, 0] - ref[:, 0]).max() / scale[i]))
+        # Realisations differ ~10x in work: the plain path's time for the whole
+        # batch is its measured seconds per amplitude-order times the batch's.
+        plain_s = sum(ts) * float(amp.sum()) / float(amp[: args.plain_sample].sum())
+        rate_b, rate_p = n / sec, n / plain_s
+        rep[int(L)] = {"realizations": n, "batched_mixed_curves_per_s": rate_b,
+                       "plain_fp64_curves_per_s": rate_p, "ratio": rate_b / rate_p,
+                       "plain_sample": args.plain_sample,
+                       "plain_scaling": "seconds per amplitude-order of the sample x the "
+                                        "batch's amplitude-orders",
+                       "echo_error_max": max(es),
+                       "fp64_routed": int((b.precisions() == abi.FP64).sum())}
+        b._destroy()
+    eng.close()
+    return rep
+
 def main(argv=None) -> None:
     ap = argparse.ArgumentParser(description="measurement runs beside the headline benchmark")
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -237,8 +289,14 @@ def main(argv=None) -> None:
     pl.add_argument("--sizes", type=int, nargs="+", default=[16, 20, 22, 24])
     pl.add_argument("--steps", type=int, default=2)
     pl.add_argument("--out", default="")
+    ps = sub.add_parser("per_size")
+    ps.add_argument("--sizes", type=int, nargs="+", default=[12, 14, 16])
+    ps.add_argument("--counts", type=int, nargs="+", default=[1184, 592, 112])
+    ps.add_argument("--plain-sample", type=int, default=4)
+    ps.add_argument("--out", default="")
     args = ap.parse_args(argv)
-    rep = {"uneven": uneven, "long": long_run, "plain": plain}[args.cmd](args)
+    rep = {"uneven": uneven, "long": long_run, "plain": plain,
+           "per_size": per_size}[args.cmd](args)
     text = json.dumps(rep, indent=1)
     print(text)
     if args.out:
