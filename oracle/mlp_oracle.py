@@ -4,7 +4,7 @@ This file is the checker for the device MLP (spin_systems_b200/csrc/mlp.cu):
 tests import it to compare forward outputs, gradients and Adam steps.  The
 product never imports it.
 
-The network is the one BASELINE's learned-surrogate workload names:
+The network is the learned-surrogate workload's:
 6 -> 256 -> 256 -> 256 -> 128, GELU (erf form) on the three hidden layers, a
 linear output layer and a mean-squared-error loss.  Everything here runs in
 float64.  With ``bf16=True`` the oracle rounds exactly where the device path

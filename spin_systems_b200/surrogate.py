@@ -215,7 +215,7 @@ class Surrogate:
 
 
 def run(args) -> dict:
-    """Generate, train, calibrate and judge; returns the report.  Each size
+    """Generate, train, calibrate and evaluate; returns the report.  Each size
     gets its own number of points (larger L costs more per curve), split
     80 / 10 / 10 into training, calibration and test points."""
     eng = Engine(0)

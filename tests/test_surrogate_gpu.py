@@ -64,7 +64,7 @@ def test_surrogate_gains_over_the_method_without_it(engine):
     t0 = time.perf_counter()
     exact = sg.exact(engine, pte, 4, mixed_order_limit=-1)
     t_exact = time.perf_counter() - t0
-    assert np.array_equal(exact, yte)           # the judge is deterministic
+    assert np.array_equal(exact, yte)           # the exact engine is deterministic
     rms = math.sqrt(((pred - yte) ** 2).mean())
     nn = sg.nearest_neighbour(ptr, ytr, pte)
     rms_nn = math.sqrt(((nn - yte) ** 2).mean())
