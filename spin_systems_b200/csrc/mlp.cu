@@ -67,6 +67,8 @@ struct GemmArgs {
   __nv_bfloat16* out_bt;   // the same, transposed ([N][M]); may be null
   const float* zin;        // BACK: pre-activation of the layer below ([M][N])
   int* flags;              // [0] set to 1 on a timed-out wait
+  int splits;              // F32 only: K split over gridDim.y CTAs per row tile
+  float* partial;          // splits > 1: [splits][M][N] FP32 slices, summed by k_splitk_sum
 };
 
 size_t gemm_smem(int N) {
@@ -233,7 +235,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
   const uint32_t tmem = *tmem_slot;
 
   const int m0 = blockIdx.x * BM;
-  const int nk = a.K / BK;
+  const int nk = a.K / BK / a.splits;      // k-tiles of this CTA's slice
+  const int kbase = blockIdx.y * nk;       // its first k-tile
 
   if (warp == 0) {
     if (lane == 0) {
@@ -249,8 +252,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         uint8_t* sa = base + s * stage_bytes;
         const uint32_t fb = smem_u32(&full[s]);
         mbar_expect_tx(fb, stage_bytes);
-        tma_load_2d(smem_u32(sa), &map_a, fb, kt * BK, m0);
-        tma_load_2d(smem_u32(sa + kABytes), &map_b, fb, kt * BK, 0);
+        tma_load_2d(smem_u32(sa), &map_a, fb, (kbase + kt) * BK, m0);
+        tma_load_2d(smem_u32(sa + kABytes), &map_b, fb, (kbase + kt) * BK, 0);
         ++issued;
       }
       if (!ok) atomicExch(&s_fail, 1);
@@ -311,7 +314,10 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
           v[4 * q + 3] *= gelu_grad(z.w);
         }
       }
-      float4* fp = reinterpret_cast<float4*>(a.out_f32 + size_t(row) * N + c0);
+      float* out = (EPI == EPI_F32 && a.splits > 1)
+                       ? a.partial + size_t(blockIdx.y) * size_t(M) * N
+                       : a.out_f32;
+      float4* fp = reinterpret_cast<float4*>(out + size_t(row) * N + c0);
 #pragma unroll
       for (int q = 0; q < 4; ++q) fp[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
       if (EPI == EPI_HIDDEN || EPI == EPI_BACK) {
@@ -336,6 +342,21 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols)
                  : "memory");
   }
+}
+
+// Sum of the split-K slices in slice order (deterministic): out = sum_s part[s].
+__global__ void k_splitk_sum(const float4* __restrict__ part, int splits, size_t n4, float4* out) {
+  const size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+  if (i >= n4) return;
+  float4 acc = part[i];
+  for (int s = 1; s < splits; ++s) {
+    const float4 v = part[size_t(s) * n4 + i];
+    acc.x += v.x;
+    acc.y += v.y;
+    acc.z += v.z;
+    acc.w += v.w;
+  }
+  out[i] = acc;
 }
 
 // ------------------------------------------------------- small kernels
@@ -571,6 +592,7 @@ struct ss_mlp {
   __nv_bfloat16* dzt[2] = {};               // [256][batch]
   double* loss_part = nullptr;
   float* col_part = nullptr;                // column-sum partials
+  float* splitk = nullptr;                  // split-K slices of the weight gradients
   double* losses = nullptr;                 // per-step losses of the last train call
   int64_t losses_cap = 0;
   int* idx = nullptr;                       // batch rows (data-set indices)
@@ -596,10 +618,9 @@ void dalloc(T** p, size_t n) {
   SS_CUDA(cudaMemset(*p, 0, sizeof(T) * std::max<size_t>(n, 1)));
 }
 
-void run_gemm(ss_mlp* n, const Gemm& gm) {
-  ss_engine* e = n->engine;
+void launch_gemm(ss_engine* e, const Gemm& gm) {
   const GemmArgs& a = gm.args;
-  const dim3 grid(a.M / BM);
+  const dim3 grid(a.M / BM, a.splits);
   const size_t smem = gemm_smem(a.N);
   switch (gm.epi) {
     case EPI_HIDDEN: launch(e, k_gemm<EPI_HIDDEN>, grid, kGemmThreads, smem, gm.ma, gm.mb, a); break;
@@ -607,6 +628,25 @@ void run_gemm(ss_mlp* n, const Gemm& gm) {
     case EPI_BACK: launch(e, k_gemm<EPI_BACK>, grid, kGemmThreads, smem, gm.ma, gm.mb, a); break;
     default: launch(e, k_gemm<EPI_F32>, grid, kGemmThreads, smem, gm.ma, gm.mb, a); break;
   }
+  if (a.splits > 1) {
+    const size_t n4 = size_t(a.M) * a.N / 4;
+    launch(e, k_splitk_sum, dim3(static_cast<unsigned>((n4 + 255) / 256)), 256, 0,
+           reinterpret_cast<const float4*>(a.partial), a.splits, n4,
+           reinterpret_cast<float4*>(a.out_f32));
+  }
+}
+
+void run_gemm(ss_mlp* n, const Gemm& gm) { launch_gemm(n->engine, gm); }
+
+// K slices for a weight-gradient product (K = the batch, long; M = a layer
+// width, one or two row tiles): enough CTAs to spread over the device with
+// at least four k-tiles each, a power of two dividing the k-tile count.
+int splitk_for(int M, int K) {
+  const int nk = K / BK;
+  const int want = std::max(1, 64 / std::max(1, M / BM));
+  int s = 1;
+  while (s * 2 <= want && nk % (s * 2) == 0 && nk / (s * 2) >= 4) s *= 2;
+  return s;
 }
 
 Gemm make_gemm(int epi, const __nv_bfloat16* A, const __nv_bfloat16* B, int M, int N, int K,
@@ -620,6 +660,7 @@ Gemm make_gemm(int epi, const __nv_bfloat16* A, const __nv_bfloat16* B, int M, i
   g.args.N = N;
   g.args.K = K;
   g.args.flags = flags;
+  g.args.splits = 1;
   g.epi = epi;
   return g;
 }
@@ -699,6 +740,7 @@ void build(ss_mlp* n) {
     const __nv_bfloat16* inT = l == 0 ? n->xt : n->ht[l - 1];  // [in][B]
     Gemm gw = make_gemm(EPI_F32, n->dzt[slot], inT, kRowsOut[l], kRowsIn[l], B, flags);
     gw.args.out_f32 = n->gw[l];
+    gw.args.splits = splitk_for(kRowsOut[l], B);
     n->bwd_w[l] = gw;
     if (l >= 1) {
       Gemm gx = make_gemm(EPI_BACK, n->dz[slot], n->wt[l], B, kRowsIn[l], kRowsOut[l], flags);
@@ -709,6 +751,14 @@ void build(ss_mlp* n) {
       n->bwd_x[l] = gx;
     }
   }
+  // one workspace for the split-K slices, shared by the (serial) products
+  size_t ws = 0;
+  for (int l = 0; l < kLayers; ++l) {
+    const GemmArgs& a = n->bwd_w[l].args;
+    if (a.splits > 1) ws = std::max(ws, size_t(a.splits) * a.M * a.N);
+  }
+  if (ws > 0) dalloc(&n->splitk, ws);
+  for (int l = 0; l < kLayers; ++l) n->bwd_w[l].args.partial = n->splitk;
 }
 
 void refresh_copies(ss_mlp* n, float lr_t, int update) {
@@ -819,7 +869,7 @@ int ss_mlp_destroy(ss_mlp* n) {
     if (n == nullptr) return;
     if (n->engine && n->engine->stream) cudaStreamSynchronize(n->engine->stream);
     void* ptrs[] = {n->p, n->m, n->v, n->x, n->xt, n->y, n->target, n->g, n->loss_part,
-                    n->col_part, n->losses, n->idx, n->data_x, n->data_y};
+                    n->col_part, n->splitk, n->losses, n->idx, n->data_x, n->data_y};
     for (void* q : ptrs) cudaFree(q);
     for (int l = 0; l < kLayers; ++l) {
       cudaFree(n->gw[l]);
@@ -1033,11 +1083,12 @@ int ss_mlp_gemm_test(ss_engine* e, const uint16_t* a, const uint16_t* b, int M, 
     SS_CUDA(cudaSetDevice(e->device));
     set_smem_attrs();
     __nv_bfloat16 *da = nullptr, *db = nullptr;
-    float* dc = nullptr;
+    float *dc = nullptr, *dp = nullptr;
     auto cleanup = [&] {
       cudaFree(da);
       cudaFree(db);
       cudaFree(dc);
+      cudaFree(dp);
     };
     try {
       SS_CUDA(cudaMalloc(&da, sizeof(uint16_t) * size_t(M) * K));
@@ -1047,7 +1098,12 @@ int ss_mlp_gemm_test(ss_engine* e, const uint16_t* a, const uint16_t* b, int M, 
       SS_CUDA(cudaMemcpyAsync(db, b, sizeof(uint16_t) * size_t(N) * K, cudaMemcpyHostToDevice, e->stream));
       Gemm g = make_gemm(EPI_F32, da, db, M, N, K, e->dev_flags + 8);
       g.args.out_f32 = dc;
-      launch(e, k_gemm<EPI_F32>, dim3(M / BM), kGemmThreads, gemm_smem(N), g.ma, g.mb, g.args);
+      g.args.splits = splitk_for(M, K);
+      if (g.args.splits > 1) {
+        SS_CUDA(cudaMalloc(&dp, sizeof(float) * size_t(g.args.splits) * M * N));
+        g.args.partial = dp;
+      }
+      launch_gemm(e, g);
       SS_CUDA(cudaMemcpyAsync(c, dc, sizeof(float) * size_t(M) * N, cudaMemcpyDeviceToHost, e->stream));
       sync(e);
       int flag = 0;
