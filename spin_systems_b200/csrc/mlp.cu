@@ -362,9 +362,11 @@ __global__ void k_splitk_sum(const float4* __restrict__ part, int splits, size_t
 // ------------------------------------------------------- small kernels
 // Builds one batch: rows of the data set named by idx (or zero rows where
 // idx < 0) as the padded BF16 input, its transpose, and the FP32 targets.
+// With `cursor` (training graphs) the batch is rows cursor[0] * rows .. of idx.
 __global__ void k_gather(const float* __restrict__ data_x, const float* __restrict__ data_y,
-                         const int* __restrict__ idx, int rows, __nv_bfloat16* x,
-                         __nv_bfloat16* xt, float* target) {
+                         const int* __restrict__ idx_base, int rows, __nv_bfloat16* x,
+                         __nv_bfloat16* xt, float* target, const int* cursor) {
+  const int* idx = cursor ? idx_base + size_t(cursor[0]) * rows : idx_base;
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r < rows) {
     const int i = idx[r];
@@ -418,12 +420,22 @@ __global__ void k_loss(const float* __restrict__ y, const float* __restrict__ t,
   }
 }
 
-// loss[slot] = sum of the block partials / (valid * kOut), in block order.
-__global__ void k_loss_total(const double* partial, int nblocks, int valid, double* loss, int slot) {
+// loss[slot] = sum of the block partials / (valid * kOut), in block order;
+// with `cursor` (training graphs) the slot is the step index cursor[1].
+__global__ void k_loss_total(const double* partial, int nblocks, int valid, double* loss, int slot,
+                             const int* cursor) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
     double s = 0.0;
     for (int b = 0; b < nblocks; ++b) s += partial[b];
-    loss[slot] = s / (double(valid) * double(kOut));
+    loss[cursor ? cursor[1] : slot] = s / (double(valid) * double(kOut));
+  }
+}
+
+// The training graph's step counter: batch position in the epoch, step index.
+__global__ void k_advance(int* cursor, int per_epoch) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    cursor[0] = (cursor[0] + 1) % per_epoch;
+    cursor[1] += 1;
   }
 }
 
@@ -474,10 +486,14 @@ struct Segs {
 
 // Adam on the FP32 master parameters (update = 1), then the BF16 copies the
 // GEMMs read.  update = 0 only refreshes the copies.
-__global__ void k_adam(Segs segs, float* p, float* m, float* v, long long total, float lr_t,
-                       float b1, float b2, float eps, int update) {
+// With `lr_steps` (training graphs) the step's learning rate is
+// lr_steps[cursor[1]].
+__global__ void k_adam(Segs segs, float* p, float* m, float* v, long long total, float lr_host,
+                       float b1, float b2, float eps, int update, const float* lr_steps,
+                       const int* cursor) {
   const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
   if (i >= total) return;
+  const float lr_t = lr_steps ? lr_steps[cursor[1]] : lr_host;
   int k = 0;
   while (k + 1 < 2 * kLayers && i >= segs.s[k + 1].off) ++k;
   const Seg& sg = segs.s[k];
@@ -593,6 +609,9 @@ struct ss_mlp {
   double* loss_part = nullptr;
   float* col_part = nullptr;                // column-sum partials
   float* splitk = nullptr;                  // split-K slices of the weight gradients
+  int* cursor = nullptr;                    // training graph: epoch position, step index
+  float* lr_steps = nullptr;                // training graph: learning rate per step
+  int64_t lr_cap = 0;
   double* losses = nullptr;                 // per-step losses of the last train call
   int64_t losses_cap = 0;
   int* idx = nullptr;                       // batch rows (data-set indices)
@@ -761,10 +780,11 @@ void build(ss_mlp* n) {
   for (int l = 0; l < kLayers; ++l) n->bwd_w[l].args.partial = n->splitk;
 }
 
-void refresh_copies(ss_mlp* n, float lr_t, int update) {
+void refresh_copies(ss_mlp* n, float lr_t, int update, const float* lr_steps = nullptr,
+                    const int* cursor = nullptr) {
   const long long total = param_count();
   launch(n->engine, k_adam, dim3(static_cast<unsigned>((total + 255) / 256)), 256, 0, n->segs,
-         n->p, n->m, n->v, total, lr_t, 0.9f, 0.999f, 1e-8f, update);
+         n->p, n->m, n->v, total, lr_t, 0.9f, 0.999f, 1e-8f, update, lr_steps, cursor);
 }
 
 void forward(ss_mlp* n, bool keep_transposes) {
@@ -786,13 +806,13 @@ void colsum(ss_mlp* n, int N, float* out) {
 
 // Backward pass of the batch in x / target (loss over the first `valid`
 // rows); writes gw, gb and the loss into losses[slot].
-void backward(ss_mlp* n, int valid, double* loss, int slot) {
+void backward(ss_mlp* n, int valid, double* loss, int slot, const int* cursor = nullptr) {
   ss_engine* e = n->engine;
   const int B = n->batch;
   const int nb = B / kGemmThreads;
   launch(e, k_loss, dim3(nb), kGemmThreads, 0, n->y, n->target, B, valid, n->g, n->dz[0],
          n->dzt[0], n->loss_part);
-  launch(e, k_loss_total, dim3(1), 32, 0, n->loss_part, nb, valid, loss, slot);
+  launch(e, k_loss_total, dim3(1), 32, 0, n->loss_part, nb, valid, loss, slot, cursor);
   colsum(n, kOut, n->gb[3]);
   for (int l = kLayers - 1; l >= 0; --l) {
     run_gemm(n, n->bwd_w[l]);
@@ -803,10 +823,11 @@ void backward(ss_mlp* n, int valid, double* loss, int slot) {
   }
 }
 
-void gather(ss_mlp* n, const float* dx, const float* dy, const int* idx) {
+void gather(ss_mlp* n, const float* dx, const float* dy, const int* idx,
+            const int* cursor = nullptr) {
   const int B = n->batch;
   launch(n->engine, k_gather, dim3(B / kGemmThreads), kGemmThreads, 0, dx, dy, idx, B, n->x,
-         n->xt, dy ? n->target : nullptr);
+         n->xt, dy ? n->target : nullptr, cursor);
 }
 
 void check_timeout(ss_mlp* n) {
@@ -869,7 +890,8 @@ int ss_mlp_destroy(ss_mlp* n) {
     if (n == nullptr) return;
     if (n->engine && n->engine->stream) cudaStreamSynchronize(n->engine->stream);
     void* ptrs[] = {n->p, n->m, n->v, n->x, n->xt, n->y, n->target, n->g, n->loss_part,
-                    n->col_part, n->splitk, n->losses, n->idx, n->data_x, n->data_y};
+                    n->col_part, n->splitk, n->cursor, n->lr_steps, n->losses, n->idx,
+                    n->data_x, n->data_y};
     for (void* q : ptrs) cudaFree(q);
     for (int l = 0; l < kLayers; ++l) {
       cudaFree(n->gw[l]);
@@ -1041,30 +1063,75 @@ int ss_mlp_train(ss_mlp* n, int64_t steps, float lr_start, float lr_end, uint64_
       n->losses_cap = steps;
     }
     const int64_t per_epoch = n->data_n / B;
+    require(per_epoch < (int64_t{1} << 30) && steps < (int64_t{1} << 31), SS_ERR_INVALID_ARGUMENT,
+            "too many steps");
+    // Learning rate per step (cosine from lr_start to lr_end) with Adam's bias
+    // correction folded in, for the graph to read by step index.
+    std::vector<float> lr(static_cast<size_t>(std::max<int64_t>(steps, 1)));
+    for (int64_t t = 0; t < steps; ++t) {
+      const double frac = steps > 1 ? double(t) / double(steps - 1) : 0.0;
+      const double base = lr_end + 0.5 * (lr_start - lr_end) * (1.0 + std::cos(3.14159265358979323846 * frac));
+      const double k = double(n->steps + t + 1);
+      const double c1 = 1.0 - std::pow(0.9, k), c2 = 1.0 - std::pow(0.999, k);
+      lr[t] = static_cast<float>(base * std::sqrt(c2) / c1);
+    }
+    if (n->lr_cap < steps) {
+      cudaFree(n->lr_steps);
+      n->lr_steps = nullptr;
+      SS_CUDA(cudaMalloc(&n->lr_steps, sizeof(float) * lr.size()));
+      n->lr_cap = steps;
+    }
+    if (!n->cursor) SS_CUDA(cudaMalloc(&n->cursor, 2 * sizeof(int)));
+    SS_CUDA(cudaMemcpyAsync(n->lr_steps, lr.data(), sizeof(float) * lr.size(), cudaMemcpyHostToDevice, e->stream));
+    SS_CUDA(cudaMemsetAsync(n->cursor, 0, 2 * sizeof(int), e->stream));
+    // One step -- gather, forward, loss, backward, Adam, advance -- captured
+    // once as a CUDA graph and replayed: the step's ~25 launches would
+    // otherwise bound it.  What changes per step (batch position, loss slot,
+    // learning rate) is read from device memory by step index.
+    cudaGraphExec_t exec = nullptr;
+    if (steps > 0) {
+      cudaGraph_t graph = nullptr;
+      SS_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+      try {
+        gather(n, n->data_x, n->data_y, n->idx, n->cursor);
+        forward(n, true);
+        backward(n, B, n->losses, 0, n->cursor);
+        refresh_copies(n, 0.0f, 1, n->lr_steps, n->cursor);
+        launch(e, k_advance, dim3(1), 32, 0, n->cursor, static_cast<int>(per_epoch));
+      } catch (...) {
+        cudaStreamEndCapture(e->stream, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        throw;
+      }
+      SS_CUDA(cudaStreamEndCapture(e->stream, &graph));
+      const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+      cudaGraphDestroy(graph);
+      SS_CUDA(ie);
+    }
     std::vector<int> perm(static_cast<size_t>(n->data_n));
     uint64_t s = seed ^ 0xBB67AE8584CAA73Bull;
-    for (int64_t t = 0; t < steps; ++t) {
-      const int64_t at = t % per_epoch;
-      if (at == 0) {
-        for (int64_t i = 0; i < n->data_n; ++i) perm[i] = static_cast<int>(i);
-        for (int64_t i = n->data_n - 1; i > 0; --i) {
-          const int64_t j = static_cast<int64_t>(mix64(s) % uint64_t(i + 1));
-          std::swap(perm[i], perm[j]);
+    try {
+      for (int64_t t = 0; t < steps; ++t) {
+        if (t % per_epoch == 0) {
+          for (int64_t i = 0; i < n->data_n; ++i) perm[i] = static_cast<int>(i);
+          for (int64_t i = n->data_n - 1; i > 0; --i) {
+            const int64_t j = static_cast<int64_t>(mix64(s) % uint64_t(i + 1));
+            std::swap(perm[i], perm[j]);
+          }
+          SS_CUDA(cudaMemcpyAsync(n->idx, perm.data(), sizeof(int) * perm.size(), cudaMemcpyHostToDevice, e->stream));
+          sync(e);  // perm is reused on the host
         }
-        SS_CUDA(cudaMemcpyAsync(n->idx, perm.data(), sizeof(int) * perm.size(), cudaMemcpyHostToDevice, e->stream));
-        sync(e);  // perm is reused on the host
+        SS_CUDA(cudaGraphLaunch(exec, e->stream));
       }
-      gather(n, n->data_x, n->data_y, n->idx + at * B);
-      forward(n, true);
-      backward(n, B, n->losses, static_cast<int>(t));
-      // cosine schedule from lr_start to lr_end, Adam bias correction
-      const double frac = steps > 1 ? double(t) / double(steps - 1) : 0.0;
-      const double lr = lr_end + 0.5 * (lr_start - lr_end) * (1.0 + std::cos(3.14159265358979323846 * frac));
-      ++n->steps;
-      const double c1 = 1.0 - std::pow(0.9, double(n->steps));
-      const double c2 = 1.0 - std::pow(0.999, double(n->steps));
-      refresh_copies(n, static_cast<float>(lr * std::sqrt(c2) / c1), 1);
+    } catch (...) {
+      if (exec) cudaGraphExecDestroy(exec);
+      throw;
     }
+    if (exec) {
+      sync(e);
+      cudaGraphExecDestroy(exec);
+    }
+    n->steps += steps;
     if (losses && steps > 0) {
       SS_CUDA(cudaMemcpyAsync(losses, n->losses, sizeof(double) * size_t(steps), cudaMemcpyDeviceToHost, e->stream));
     }
