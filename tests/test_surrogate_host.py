@@ -48,3 +48,18 @@ def test_error_model_takes_the_worst_near_calibration_point():
     far = p[[5]].copy()
     far["nspins"] = 12
     assert np.isinf(s.estimate_error(far)[0])
+
+
+def test_vectorised_nearest_matches_brute_force():
+    rng = np.random.default_rng(4)
+    ref = rng.normal(size=(300, 4))
+    q = rng.normal(size=(1000, 4))
+    got = sg._nearest(ref, q, 5, chunk=128)
+    d = ((q[:, None, :] - ref[None, :, :]) ** 2).sum(axis=2)
+    want = np.sort(d, axis=1)[:, :5]
+    assert np.allclose(np.sort(np.take_along_axis(d, got, axis=1), axis=1), want)
+    one = sg._nearest(ref, q, 1)[:, 0]
+    assert np.array_equal(one, d.argmin(axis=1))
+    # fewer reference rows than k: every row, padded with the last index
+    small = sg._nearest(ref[:3], q[:7], 5)
+    assert small.shape == (7, 5) and set(np.unique(small)) <= {0, 1, 2}
