@@ -357,6 +357,13 @@ int ss_schedule_clear(void);
 int ss_schedule_describe(char* buf, size_t cap, size_t* needed);
 /* Every compiled schedule: "name threads shared_bytes" per line. */
 int ss_batch_variants(char* buf, size_t cap, size_t* needed);
+/* Split-cluster schedules (names ending ".split") run the state and the
+ * reference of a realisation on clusters of their own and keep both vectors
+ * at every measurement point; a bucket runs in launches whose snapshots fit
+ * `bytes` of device memory (default 16 GiB), or with the paired schedule of
+ * its size when fewer than 64 realisations (or the whole bucket) would fit.
+ * Process-wide; applies to batches created afterwards.  bytes >= 0. */
+int ss_set_snapshot_budget(int64_t bytes);
 
 /* -------------------------------------------------------- echo surrogate
  * No counterpart in the reference (its parameter sweeps always run the

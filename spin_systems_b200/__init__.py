@@ -629,6 +629,14 @@ def clear_schedule() -> None:
     check(load().ss_schedule_clear())
 
 
+def set_snapshot_budget(nbytes: int) -> None:
+    """ss_set_snapshot_budget: device memory one launch of a split-cluster
+    schedule may hold in measurement snapshots (default 16 GiB)."""
+    lib = load()
+    lib.ss_set_snapshot_budget.argtypes = [C.c_int64]
+    check(lib.ss_set_snapshot_budget(int(nbytes)))
+
+
 def tune(engine: Engine, cfg: SsRunConfig, first: int = 0, sample: int = 64,
          precision: int = abi.MIXED, cache=None):
     """ss_batch_tune: time every candidate schedule of the config's sizes and

@@ -7,6 +7,7 @@
 // batch_kernel.cuh.
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <cmath>
 #include <fstream>
 #include <map>
@@ -33,6 +34,10 @@ constexpr int kPrepThreads = 256;
 constexpr int kClusterSize = 2;  // state and reference of one realisation
 // Time of an FP64 amplitude-order relative to a mixed one (B200, L = 12).
 constexpr double kFp64CostFactor = 1.45;
+// Split clusters: device memory for the snapshots of one launch, and the
+// fewest realisations a launch must hold for the split schedule to be used.
+std::atomic<int64_t> g_snap_budget{int64_t{16} << 30};
+constexpr size_t kSnapMinSlots = 64;
 
 // ---------------------------------------------------------------- device
 __device__ __forceinline__ double2 sigma_at(const double2* in, uint32_t k, int s, int axis) {
@@ -279,6 +284,92 @@ __device__ void pulse_op(const Args& args, int L, double2* st, const Op& op, int
   }
 }
 
+// One thread's share of observable i of a realisation with state psi and
+// reference ref: amplitudes k0 + threadIdx.x, k0 + threadIdx.x + NT, ... < k1.
+// CORR (x, y) = <ref| sum_s sigma^axis_s |psi>, MAG = <psi|sigma^axis_spin|psi>,
+// NORM = (<psi|psi>, <ref|ref>), ENERGY = <psi|H|psi> with the realisation's
+// own fields, all in FP64.
+template <int NT>
+__device__ __forceinline__ double2 obs_thread(const Args& args, const RealDev& rd, int L,
+                                              const double2* psi, const double2* ref, int i,
+                                              uint32_t k0, uint32_t k1) {
+  const int kind = args.obs[3 * i], axis = args.obs[3 * i + 1], spin = args.obs[3 * i + 2];
+  double2 v = make_double2(0.0, 0.0);
+  if (kind == SS_OBS_CORR) {
+    for (uint32_t k = k0 + threadIdx.x; k < k1; k += NT) {
+      double sr = 0.0, si = 0.0;
+      for (int s = 0; s < L; ++s) {
+        const double2 q = sigma_at(psi, k, s, axis);
+        sr += q.x;
+        si += q.y;
+      }
+      const double2 r = ref[k];
+      v.x += r.x * sr + r.y * si;
+      v.y += r.x * si - r.y * sr;
+    }
+  } else if (kind == SS_OBS_MAG) {
+    for (uint32_t k = k0 + threadIdx.x; k < k1; k += NT) {
+      const double2 q = sigma_at(psi, k, spin, axis);
+      const double2 p = psi[k];
+      v.x += p.x * q.x + p.y * q.y;
+    }
+  } else if (kind == SS_OBS_NORM) {
+    for (uint32_t k = k0 + threadIdx.x; k < k1; k += NT) {
+      const double2 p = psi[k], r = ref[k];
+      v.x += p.x * p.x + p.y * p.y;
+      v.y += r.x * r.x + r.y * r.y;
+    }
+  } else {
+    const TypeDev ty = args.types[rd.type_off + args.measure_type];
+    const double* cb = args.cpool + ty.c_off;
+    const int2* pl = args.pairs + rd.pair_off;
+    const int P = rd.npairs;
+    for (uint32_t k = k0 + threadIdx.x; k < k1; k += NT) {
+      const double2 p = psi[k];
+      double d = 0.0;
+      for (int s = 0; s < L; ++s) d += ((k >> s) & 1u) ? cb[3 * P + s] : -cb[3 * P + s];
+      for (int q = 0; q < P; ++q) {
+        const int2 pr = pl[q];
+        d += (((k >> pr.x) ^ (k >> pr.y)) & 1u) ? -cb[2 * P + q] : cb[2 * P + q];
+      }
+      double hr = d * p.x, hi = d * p.y;
+      for (int s = 0; s < L; ++s) {
+        const double cx = cb[3 * P + L + s];
+        const double cy = ((k >> s) & 1u) ? -cb[3 * P + 2 * L + s] : cb[3 * P + 2 * L + s];
+        const double2 w = psi[k ^ (1u << s)];
+        hr += cx * w.x - cy * w.y;
+        hi += cx * w.y + cy * w.x;
+      }
+      for (int q = 0; q < P; ++q) {
+        const int2 pr = pl[q];
+        const bool anti = (((k >> pr.x) ^ (k >> pr.y)) & 1u) != 0;
+        const double c = anti ? cb[q] : cb[P + q];
+        const double2 w = psi[k ^ (1u << pr.x) ^ (1u << pr.y)];
+        hr += c * w.x;
+        hi += c * w.y;
+      }
+      v.x += hr * p.x + hi * p.y;
+    }
+  }
+  return v;
+}
+
+// Writes observable i's total into the row at column col and returns the
+// next column (CORR and NORM take two).
+__device__ __forceinline__ int obs_store(const Args& args, double* row, int col, int i, double2 v) {
+  const int kind = args.obs[3 * i];
+  if (kind == SS_OBS_CORR) {
+    row[col] = v.x;
+    row[col + 1] = v.y;
+  } else if (kind == SS_OBS_NORM) {
+    row[col] = sqrt(v.x);
+    row[col + 1] = sqrt(v.y);
+  } else {
+    row[col] = v.x;
+  }
+  return col + ((kind == SS_OBS_CORR || kind == SS_OBS_NORM) ? 2 : 1);
+}
+
 template <int L, int NT>
 __device__ void measure_op(const Args& args, double2* stage, double2* red, const RealDev& rd,
                            const double2* st, const Op& op) {
@@ -291,77 +382,8 @@ __device__ void measure_op(const Args& args, double2* stage, double2* red, const
   double* row = args.rows + rd.row_off + static_cast<long long>(op.a) * args.width;
   int col = 0;
   for (int i = 0; i < args.nobs; ++i) {
-    const int kind = args.obs[3 * i], axis = args.obs[3 * i + 1], spin = args.obs[3 * i + 2];
-    double2 v = make_double2(0.0, 0.0);
-    if (kind == SS_OBS_CORR) {
-      for (uint32_t k = t; k < N; k += NT) {
-        double sr = 0.0, si = 0.0;
-        for (int s = 0; s < L; ++s) {
-          const double2 q = sigma_at(stage, k, s, axis);
-          sr += q.x;
-          si += q.y;
-        }
-        const double2 r = ref[k];
-        v.x += r.x * sr + r.y * si;
-        v.y += r.x * si - r.y * sr;
-      }
-    } else if (kind == SS_OBS_MAG) {
-      for (uint32_t k = t; k < N; k += NT) {
-        const double2 q = sigma_at(stage, k, spin, axis);
-        const double2 p = stage[k];
-        v.x += p.x * q.x + p.y * q.y;
-      }
-    } else if (kind == SS_OBS_NORM) {
-      for (uint32_t k = t; k < N; k += NT) {
-        const double2 p = stage[k], r = ref[k];
-        v.x += p.x * p.x + p.y * p.y;
-        v.y += r.x * r.x + r.y * r.y;
-      }
-    } else {  // energy with the realisation's own fields, FP64
-      const TypeDev ty = args.types[rd.type_off + args.measure_type];
-      const double* cb = args.cpool + ty.c_off;
-      const int2* pl = args.pairs + rd.pair_off;
-      const int P = rd.npairs;
-      for (uint32_t k = t; k < N; k += NT) {
-        const double2 p = stage[k];
-        double d = 0.0;
-        for (int s = 0; s < L; ++s) d += ((k >> s) & 1u) ? cb[3 * P + s] : -cb[3 * P + s];
-        for (int q = 0; q < P; ++q) {
-          const int2 pr = pl[q];
-          d += (((k >> pr.x) ^ (k >> pr.y)) & 1u) ? -cb[2 * P + q] : cb[2 * P + q];
-        }
-        double hr = d * p.x, hi = d * p.y;
-        for (int s = 0; s < L; ++s) {
-          const double cx = cb[3 * P + L + s];
-          const double cy = ((k >> s) & 1u) ? -cb[3 * P + 2 * L + s] : cb[3 * P + 2 * L + s];
-          const double2 w = stage[k ^ (1u << s)];
-          hr += cx * w.x - cy * w.y;
-          hi += cx * w.y + cy * w.x;
-        }
-        for (int q = 0; q < P; ++q) {
-          const int2 pr = pl[q];
-          const bool anti = (((k >> pr.x) ^ (k >> pr.y)) & 1u) != 0;
-          const double c = anti ? cb[q] : cb[P + q];
-          const double2 w = stage[k ^ (1u << pr.x) ^ (1u << pr.y)];
-          hr += c * w.x;
-          hi += c * w.y;
-        }
-        v.x += hr * p.x + hi * p.y;
-      }
-    }
-    v = cta_sum2<NT>(v, red);
-    if (t == 0) {
-      if (kind == SS_OBS_CORR) {
-        row[col] = v.x;
-        row[col + 1] = v.y;
-      } else if (kind == SS_OBS_NORM) {
-        row[col] = sqrt(v.x);
-        row[col + 1] = sqrt(v.y);
-      } else {
-        row[col] = v.x;
-      }
-    }
-    col += (kind == SS_OBS_CORR || kind == SS_OBS_NORM) ? 2 : 1;
+    const double2 v = cta_sum2<NT>(obs_thread<NT>(args, rd, L, stage, ref, i, 0u, N), red);
+    if (t == 0) col = obs_store(args, row, col, i, v);
   }
   __syncthreads();
 }
@@ -454,6 +476,15 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(Geo<L, R>::NT)
 // cluster barrier per Chebyshev order publishes T_n to the peers.  The
 // cluster holds 2C CTAs: ranks 0 .. C-1 the state, C .. 2C-1 the reference;
 // both run the same number of orders, so their barriers pair up.
+//
+// Split clusters hold C CTAs and carry one vector: a work item is a
+// (realisation, vector) pair, so the state and the reference of a
+// realisation run on different clusters and never wait for each other.  At
+// each measurement point a vector copies itself to its snapshot slot, and
+// k_batch_measure_snap computes the observables from the snapshot pairs once
+// the bucket is done.  Half the cluster size lets more CTAs be resident (at
+// L = 16: 18 clusters of 8 instead of 7 of 16), for one vector write and
+// read per measurement point.
 namespace cg = cooperative_groups;
 
 template <typename T>
@@ -475,7 +506,7 @@ __device__ void evolve_dist(const Args& args, const Smem<Real>& sm, const RealDe
   constexpr bool kMixed = std::is_same<Real, float>::value;
   const uint32_t t = threadIdx.x;
   const unsigned me = cl.block_rank();
-  const unsigned group = static_cast<unsigned>(vec) * C;
+  const unsigned group = me - part;  // cluster rank of this vector's part 0
   const uint32_t hi = part << Ll;
   const int P = rd.npairs;
   const double* cb = args.cpool + ty.c_off;
@@ -708,89 +739,18 @@ __device__ void measure_dist(const Args& args, double2* red, double2* s_part, co
   const unsigned me = cl.block_rank(), nb = cl.num_blocks();
   const uint32_t chunk = N / nb;
   const uint32_t k0 = me * chunk, k1 = k0 + chunk;
-  const uint32_t t = threadIdx.x;
-  const double2* psi = st;
-  const double2* ref = st + N;
   for (int i = 0; i < args.nobs; ++i) {
-    const int kind = args.obs[3 * i], axis = args.obs[3 * i + 1], spin = args.obs[3 * i + 2];
-    double2 v = make_double2(0.0, 0.0);
-    if (kind == SS_OBS_CORR) {
-      for (uint32_t k = k0 + t; k < k1; k += NT) {
-        double sr = 0.0, si = 0.0;
-        for (int s = 0; s < L; ++s) {
-          const double2 q = sigma_at(psi, k, s, axis);
-          sr += q.x;
-          si += q.y;
-        }
-        const double2 r = ref[k];
-        v.x += r.x * sr + r.y * si;
-        v.y += r.x * si - r.y * sr;
-      }
-    } else if (kind == SS_OBS_MAG) {
-      for (uint32_t k = k0 + t; k < k1; k += NT) {
-        const double2 q = sigma_at(psi, k, spin, axis);
-        const double2 p = psi[k];
-        v.x += p.x * q.x + p.y * q.y;
-      }
-    } else if (kind == SS_OBS_NORM) {
-      for (uint32_t k = k0 + t; k < k1; k += NT) {
-        const double2 p = psi[k], r = ref[k];
-        v.x += p.x * p.x + p.y * p.y;
-        v.y += r.x * r.x + r.y * r.y;
-      }
-    } else {
-      const TypeDev ty = args.types[rd.type_off + args.measure_type];
-      const double* cb = args.cpool + ty.c_off;
-      const int2* pl = args.pairs + rd.pair_off;
-      const int P = rd.npairs;
-      for (uint32_t k = k0 + t; k < k1; k += NT) {
-        const double2 p = psi[k];
-        double d = 0.0;
-        for (int s = 0; s < L; ++s) d += ((k >> s) & 1u) ? cb[3 * P + s] : -cb[3 * P + s];
-        for (int q = 0; q < P; ++q) {
-          const int2 pr = pl[q];
-          d += (((k >> pr.x) ^ (k >> pr.y)) & 1u) ? -cb[2 * P + q] : cb[2 * P + q];
-        }
-        double hr = d * p.x, hi = d * p.y;
-        for (int s = 0; s < L; ++s) {
-          const double cx = cb[3 * P + L + s];
-          const double cy = ((k >> s) & 1u) ? -cb[3 * P + 2 * L + s] : cb[3 * P + 2 * L + s];
-          const double2 w = psi[k ^ (1u << s)];
-          hr += cx * w.x - cy * w.y;
-          hi += cx * w.y + cy * w.x;
-        }
-        for (int q = 0; q < P; ++q) {
-          const int2 pr = pl[q];
-          const bool anti = (((k >> pr.x) ^ (k >> pr.y)) & 1u) != 0;
-          const double c = anti ? cb[q] : cb[P + q];
-          const double2 w = psi[k ^ (1u << pr.x) ^ (1u << pr.y)];
-          hr += c * w.x;
-          hi += c * w.y;
-        }
-        v.x += hr * p.x + hi * p.y;
-      }
-    }
-    v = cta_sum2<NT>(v, red);
-    if (t == 0) s_part[i] = v;
+    const double2 v = cta_sum2<NT>(obs_thread<NT>(args, rd, L, st, st + N, i, k0, k1), red);
+    if (threadIdx.x == 0) s_part[i] = v;
   }
   cl.sync();
-  if (me == 0 && t == 0) {
+  if (me == 0 && threadIdx.x == 0) {
     double* row = args.rows + rd.row_off + static_cast<long long>(op.a) * args.width;
     int col = 0;
     for (int i = 0; i < args.nobs; ++i) {
-      const int kind = args.obs[3 * i];
       double2 v = make_double2(0.0, 0.0);
       for (unsigned b = 0; b < nb; ++b) v += *peer_ptr(cl, &s_part[i], b, me);
-      if (kind == SS_OBS_CORR) {
-        row[col] = v.x;
-        row[col + 1] = v.y;
-      } else if (kind == SS_OBS_NORM) {
-        row[col] = sqrt(v.x);
-        row[col + 1] = sqrt(v.y);
-      } else {
-        row[col] = v.x;
-      }
-      col += (kind == SS_OBS_CORR || kind == SS_OBS_NORM) ? 2 : 1;
+      col = obs_store(args, row, col, i, v);
     }
   }
   cl.sync();  // partial slots may be reused
@@ -816,8 +776,9 @@ struct DistLayout {
   static constexpr size_t total = at_norm + 16;
 };
 
-// One realisation per cluster of 2 * 2^CB CTAs (cluster size given at launch).
-template <int L, int R, int CB, typename Real>
+// One realisation per cluster of 2 * 2^CB CTAs, or with SPLIT one vector per
+// cluster of 2^CB CTAs (cluster size given at launch).
+template <int L, int R, int CB, typename Real, bool SPLIT>
 __global__ void __launch_bounds__(Geo<L - CB, R>::NT) k_batch_dist(const __grid_constant__ Args args) {
   constexpr int Ll = L - CB, C = 1 << CB;
   using Gm = Geo<Ll, R>;
@@ -842,37 +803,75 @@ __global__ void __launch_bounds__(Geo<L - CB, R>::NT) k_batch_dist(const __grid_
   sm.red = reinterpret_cast<double2*>(smem_raw + DL::at_red);
   double2* s_part = reinterpret_cast<double2*>(smem_raw + DL::at_part);
   double* s_norm = reinterpret_cast<double*>(smem_raw + DL::at_norm);
-  __shared__ int s_work;
+  __shared__ int s_work, s_item;
   cg::cluster_group cluster = cg::this_cluster();
   const unsigned rank = cluster.block_rank();
-  const int vec = static_cast<int>(rank / C);
   const uint32_t part = rank % C;
+  // a split cluster's work item, re-read from shared memory where it is
+  // needed rather than held in registers across the recursion
+  const volatile int* item = &s_item;
   int* lead_work = cluster.map_shared_rank(&s_work, 0);
+  const int nitems = SPLIT ? 2 * args.nwork : args.nwork;
 
   for (;;) {
     if (rank == 0 && threadIdx.x == 0) s_work = static_cast<int>(atomicAdd(args.counter, 1u));
     cluster.sync();
     const int w = *lead_work;
+    if (SPLIT && threadIdx.x == 0) s_item = w;
     cluster.sync();
-    if (w >= args.nwork) break;
-    const RealDev rd = args.reals[args.work[w]];
+    if (w >= nitems) break;
+    const RealDev rd = args.reals[args.work[SPLIT ? w >> 1 : w]];
     double2* st = args.states + rd.state_off;
     for (int i = args.op_begin; i < args.op_end; ++i) {
       const Op op = args.ops[i];
       if (op.kind == OP_EVOLVE) {
         const TypeDev ty = args.types[rd.type_off + op.a];
         if (ty.order > 0 && op.b > 0) {
+          const int vec = SPLIT ? (*item & 1) : static_cast<int>(rank / C);
           evolve_dist<L, R, CB, Real>(args, sm, rd, st, op, ty, vec, part, cluster, s_norm);
           __threadfence();
           cluster.sync();  // psi complete in global memory
         }
       } else if (op.kind == OP_PULSE) {
+        const int vec = SPLIT ? (*item & 1) : static_cast<int>(rank / C);
         pulse_dist<NT, C>(args, L, st, op, vec, part, rd.rot_off, cluster);
+      } else if (SPLIT) {
+        // evolve and pulse end on a fenced cluster barrier, so every part
+        // of the vector is in global memory; each CTA copies its own part
+        constexpr uint32_t N = 1u << L, chunk = N / C;
+        const int slot = *item >> 1, vec = *item & 1;
+        const double2* src = st + vec * N + part * chunk;
+        double2* dst = args.snap + ((static_cast<long long>(slot) * args.nmeas + op.a) * 2 + vec) * N +
+                       part * chunk;
+        for (uint32_t k = threadIdx.x; k < chunk; k += NT) __stcg(&dst[k], __ldcg(&src[k]));
+        cluster.sync();  // no part is overwritten before its copy is taken
       } else {
         __threadfence();
         cluster.sync();
         measure_dist<NT>(args, sm.red, s_part, rd, st, op, cluster);
       }
+    }
+  }
+}
+
+// Observables from the snapshots of split clusters: one CTA per (work slot,
+// measurement point), the same per-thread sums as the one-CTA kernel.
+constexpr int kSnapThreads = 256;
+
+__global__ void __launch_bounds__(kSnapThreads) k_batch_measure_snap(const __grid_constant__ Args args) {
+  __shared__ double2 red[32];
+  const long long items = static_cast<long long>(args.nwork) * args.nmeas;
+  for (long long it = blockIdx.x; it < items; it += gridDim.x) {
+    const int slot = static_cast<int>(it / args.nmeas), m = static_cast<int>(it % args.nmeas);
+    const RealDev rd = args.reals[args.work[slot]];
+    const uint32_t N = 1u << rd.L;
+    const double2* psi = args.snap + it * 2 * N;
+    double* row = args.rows + rd.row_off + static_cast<long long>(m) * args.width;
+    int col = 0;
+    for (int i = 0; i < args.nobs; ++i) {
+      const double2 v =
+          cta_sum2<kSnapThreads>(obs_thread<kSnapThreads>(args, rd, rd.L, psi, psi + N, i, 0u, N), red);
+      if (threadIdx.x == 0) col = obs_store(args, row, col, i, v);
     }
   }
 }
@@ -886,19 +885,20 @@ struct Variant {
   size_t smem;
   void (*kernel)(Args);
   int cb;  // each vector spread over 2^cb CTAs (k_batch_dist); 0 = one CTA
-  int cluster() const { return 2 << cb; }
+  bool split;  // one vector per cluster, observables from snapshots
+  int cluster() const { return split ? 1 << cb : 2 << cb; }
 };
 
 template <int L, int R, typename Real, int PSI>
 Variant make_variant() {
   return Variant{L, R, std::is_same<Real, float>::value, PSI, Geo<L, R>::NT,
-                 SmemLayout<L, R, Real, PSI>::total, &k_batch<L, R, Real, PSI>, 0};
+                 SmemLayout<L, R, Real, PSI>::total, &k_batch<L, R, Real, PSI>, 0, false};
 }
 
-template <int L, int R, int CB, typename Real>
+template <int L, int R, int CB, typename Real, bool SPLIT = false>
 Variant make_dist_variant() {
   return Variant{L, R, std::is_same<Real, float>::value, PSI_GLOBAL, Geo<L - CB, R>::NT,
-                 DistLayout<L, R, CB, Real>::total, &k_batch_dist<L, R, CB, Real>, CB};
+                 DistLayout<L, R, CB, Real>::total, &k_batch_dist<L, R, CB, Real, SPLIT>, CB, SPLIT};
 }
 
 // The per-size schedules: register bits R and where psi lives.  Chosen so a
@@ -937,6 +937,10 @@ const std::vector<Variant>& variants() {
       make_variant<12, 3, double, PSI_REG>(),   make_variant<12, 4, double, PSI_REG>(),
       make_variant<11, 4, float, PSI_REG>(),    make_variant<10, 4, float, PSI_REG>(),
       make_variant<10, 3, double, PSI_REG>(),   make_variant<11, 3, double, PSI_REG>(),
+      // split clusters: the state and the reference of a realisation on
+      // clusters of their own
+      make_dist_variant<14, 4, 1, float, true>(), make_dist_variant<15, 4, 2, float, true>(),
+      make_dist_variant<16, 4, 3, float, true>(),
   };
   return v;
 }
@@ -952,7 +956,7 @@ const Variant* find_variant(int L, bool mixed) {
 std::string variant_name(const Variant& v) {
   static const char* homes[] = {"reg", "smem", "global"};
   return "L" + std::to_string(v.L) + ".R" + std::to_string(v.R) + (v.mixed ? ".f32." : ".f64.") +
-         homes[v.psi] + ".c" + std::to_string(1 << v.cb);
+         homes[v.psi] + ".c" + std::to_string(1 << v.cb) + (v.split ? ".split" : "");
 }
 
 }  // namespace
@@ -1014,6 +1018,9 @@ struct Bucket {
   unsigned int* counter = nullptr;
   int* dev_work = nullptr;
   cudaStream_t side = nullptr;
+  // split clusters: realisations per launch and their snapshots
+  int chunk = 0;
+  double2* snap = nullptr;
 };
 
 }  // namespace batch
@@ -1456,9 +1463,22 @@ void build_plan(ss_batch* b, const ss_run_config& c) {
            std::string("the batched engine covers L = 6..") + (mixed ? "16" : "15") +
                " in this precision; got L = " + std::to_string(L));
     }
-    // The cluster kernel's measurement keeps one partial sum per observable
-    // in a fixed shared slot array.
-    require(bk.var->cb == 0 || b->obs.size() / 3 <= static_cast<size_t>(kMaxDistObs),
+    // Split clusters keep both vectors of every realisation of a launch at
+    // every measurement point; the bucket runs in launches of `chunk`
+    // realisations within the snapshot budget, or with the paired schedule
+    // when too few fit.
+    if (bk.var->split) {
+      const size_t per_slot = b->times.size() * 2 * (size_t{1} << L) * sizeof(double2);
+      const size_t fit = per_slot > 0 ? static_cast<size_t>(g_snap_budget.load()) / per_slot : list.size();
+      if (fit < std::min(list.size(), kSnapMinSlots)) {
+        bk.var = find_variant(L, mixed);
+      } else {
+        bk.chunk = static_cast<int>(std::min(fit, list.size()));
+      }
+    }
+    // The paired cluster kernel's measurement keeps one partial sum per
+    // observable in a fixed shared slot array.
+    require(bk.var->cb == 0 || bk.var->split || b->obs.size() / 3 <= static_cast<size_t>(kMaxDistObs),
             SS_ERR_CONFIG, "sizes above 13 spins (FP32) / 12 (FP64) measure at most 8 observables");
     std::stable_sort(list.begin(), list.end(),
                      [&](int x, int y) { return per[x].cost > per[y].cost; });
@@ -1508,7 +1528,8 @@ void build_plan(ss_batch* b, const ss_run_config& c) {
     require(resident > 0, SS_ERR_RUNTIME, "batched kernel cluster does not fit the device");
     const double share = total_weight > 0.0 ? weight[i] / total_weight : 1.0;
     int clusters = static_cast<int>(share * resident);
-    clusters = std::max(1, std::min<int>(clusters, static_cast<int>(bk.work.size())));
+    const int items = bk.var->split ? 2 * bk.chunk : static_cast<int>(bk.work.size());
+    clusters = std::max(1, std::min(clusters, items));
     bk.grid = (bk.var->cb > 0 ? bk.var->cluster() : kClusterSize) * clusters;
   }
 }
@@ -1534,7 +1555,6 @@ void capture(ss_batch* b) {
         ks = bk.side;
         SS_CUDA(cudaStreamWaitEvent(ks, fork, 0));
       }
-      SS_CUDA(cudaMemsetAsync(bk.counter, 0, sizeof(unsigned int), ks));
       Args a{};
       a.ops = b->d_ops;
       a.op_begin = 0;
@@ -1555,26 +1575,44 @@ void capture(ss_batch* b) {
       a.width = static_cast<int>(b->width);
       a.measure_type = b->ntypes;
       a.flags = b->d_flags;
-      if (bk.var->cb > 0) {
-        // vectors over clusters: the cluster size is a launch attribute
-        cudaLaunchConfig_t lc{};
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = static_cast<unsigned>(bk.var->cluster());
-        attr[0].val.clusterDim.y = 1;
-        attr[0].val.clusterDim.z = 1;
-        lc.gridDim = dim3(bk.grid);
-        lc.blockDim = dim3(bk.var->threads);
-        lc.dynamicSmemBytes = bk.var->smem;
-        lc.stream = ks;
-        lc.attrs = attr;
-        lc.numAttrs = 1;
-        SS_CUDA(cudaLaunchKernelEx(&lc, bk.var->kernel, a));
-      } else {
-        bk.var->kernel<<<bk.grid, bk.var->threads, bk.var->smem, ks>>>(a);
+      a.snap = bk.snap;
+      a.nmeas = static_cast<int>(b->times.size());
+      // one launch for the bucket, or launches of `chunk` realisations
+      // (split clusters), each followed by its snapshot measurement
+      const int total = static_cast<int>(bk.work.size());
+      const int step = bk.var->split ? bk.chunk : total;
+      for (int c0 = 0; c0 < total; c0 += step) {
+        a.work = bk.dev_work + c0;
+        a.nwork = std::min(step, total - c0);
+        SS_CUDA(cudaMemsetAsync(bk.counter, 0, sizeof(unsigned int), ks));
+        if (bk.var->cb > 0) {
+          // vectors over clusters: the cluster size is a launch attribute
+          cudaLaunchConfig_t lc{};
+          cudaLaunchAttribute attr[1];
+          attr[0].id = cudaLaunchAttributeClusterDimension;
+          attr[0].val.clusterDim.x = static_cast<unsigned>(bk.var->cluster());
+          attr[0].val.clusterDim.y = 1;
+          attr[0].val.clusterDim.z = 1;
+          lc.gridDim = dim3(bk.grid);
+          lc.blockDim = dim3(bk.var->threads);
+          lc.dynamicSmemBytes = bk.var->smem;
+          lc.stream = ks;
+          lc.attrs = attr;
+          lc.numAttrs = 1;
+          SS_CUDA(cudaLaunchKernelEx(&lc, bk.var->kernel, a));
+        } else {
+          bk.var->kernel<<<bk.grid, bk.var->threads, bk.var->smem, ks>>>(a);
+        }
+        SS_CUDA(cudaGetLastError());
+        ++launches;
+        if (bk.var->split && a.nmeas > 0) {
+          const long long items = static_cast<long long>(a.nwork) * a.nmeas;
+          const unsigned grid = static_cast<unsigned>(std::min<long long>(items, 8LL * e->sm_count));
+          k_batch_measure_snap<<<grid, kSnapThreads, 0, ks>>>(a);
+          SS_CUDA(cudaGetLastError());
+          ++launches;
+        }
       }
-      SS_CUDA(cudaGetLastError());
-      ++launches;
       if (i > 0) {
         cudaEvent_t j;
         SS_CUDA(cudaEventCreateWithFlags(&j, cudaEventDisableTiming));
@@ -1658,6 +1696,7 @@ void release(ss_batch* b) {
   for (Bucket& bk : b->buckets) {
     cudaFree(bk.counter);
     cudaFree(bk.dev_work);
+    cudaFree(bk.snap);
     if (bk.side) cudaStreamDestroy(bk.side);
   }
 }
@@ -1700,6 +1739,9 @@ int ss_batch_create(ss_engine* engine, const ss_run_config* config, uint64_t fir
       for (Bucket& bk : b->buckets) {
         dev_alloc(&bk.counter, 1);
         dev_alloc(&bk.dev_work, bk.work.size());
+        if (bk.var->split) {
+          dev_alloc(&bk.snap, static_cast<size_t>(bk.chunk) * b->times.size() * 2 * (size_t{1} << bk.L));
+        }
         SS_CUDA(cudaStreamCreateWithFlags(&bk.side, cudaStreamNonBlocking));
       }
     } catch (...) {
@@ -1968,6 +2010,13 @@ int ss_schedule_clear(void) {
   return guarded([&] {
     std::lock_guard<std::mutex> lk(g_sched_mu);
     g_sched.clear();
+  });
+}
+
+int ss_set_snapshot_budget(int64_t bytes) {
+  return guarded([&] {
+    require(bytes >= 0, SS_ERR_INVALID_ARGUMENT, "the snapshot budget is a byte count");
+    g_snap_budget.store(bytes);
   });
 }
 

@@ -90,6 +90,8 @@ struct Args {
   int nobs, width;
   int measure_type;     // slot of the energy table in each realisation's types
   int* flags;           // [0]: zero norm under autonormalisation
+  double2* snap;        // split clusters: both vectors of every work slot at
+  int nmeas;            // each of the nmeas measurement points
 };
 
 template <typename Real>

@@ -27,7 +27,7 @@ from pathlib import Path
 
 import numpy as np
 
-from . import Batch, Engine, abi, realization_setup, run_realization, tune
+from . import Batch, Engine, abi, realization_setup, run_realization, schedule, tune
 from . import workloads
 
 
@@ -263,7 +263,9 @@ def per_size(args) -> dict:
                        "plain_scaling": "seconds per amplitude-order of the sample x the "
                                         "batch's amplitude-orders",
                        "echo_error_max": max(es),
-                       "fp64_routed": int((b.precisions() == abi.FP64).sum())}
+                       "fp64_routed": int((b.precisions() == abi.FP64).sum()),
+                       "schedule": {r["precision"]: r["variant"] for r in schedule()
+                                    if r["L"] == L}}
         b._destroy()
     eng.close()
     return rep

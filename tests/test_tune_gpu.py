@@ -41,7 +41,9 @@ def test_tuner_fills_the_table_and_writes_the_cache(engine, tmp_path):
                                      "L12.R4.f32.reg.c1", "L12.R3.f64.reg.c1",
                                      "L12.R4.f64.reg.c1", "L11.R4.f32.reg.c1",
                                      "L10.R4.f32.reg.c1", "L10.R3.f64.reg.c1",
-                                     "L11.R3.f64.reg.c1"])
+                                     "L11.R3.f64.reg.c1", "L14.R4.f32.global.c2.split",
+                                     "L15.R4.f32.global.c4.split",
+                                     "L16.R4.f32.global.c8.split"])
 def test_every_alternative_schedule_matches_the_oracle(engine, port, tmp_path, variant):
     ss.clear_schedule()
     spec = _spec()

@@ -15,6 +15,9 @@ def test_every_size_has_a_default_and_the_alternatives_are_listed():
     for L in (10, 11, 12, 13, 14, 15, 16):
         assert sum(n.startswith(f"L{L}.") and ".f32." in n for n in names) >= 2
     assert "L16.R4.f32.global.c8" in names
+    # state and reference on clusters of their own at the cluster sizes
+    assert {"L14.R4.f32.global.c2.split", "L15.R4.f32.global.c4.split",
+            "L16.R4.f32.global.c8.split"} <= set(names)
     for name, threads, smem in ss.variants():
         assert 32 <= threads <= 1024 and smem <= 232448
 
@@ -41,3 +44,11 @@ def test_malformed_cache_is_a_config_error(tmp_path):
     ss.clear_schedule()
     with pytest.raises(ss.InvalidArgumentError):
         ss.load_schedule(tmp_path / "missing.tsv")
+
+
+def test_snapshot_budget_is_a_byte_count():
+    with pytest.raises(ss.SpinsimError) as e:
+        ss.set_snapshot_budget(-1)
+    assert e.value.kind == "invalid_argument"
+    ss.set_snapshot_budget(0)
+    ss.set_snapshot_budget(16 << 30)
