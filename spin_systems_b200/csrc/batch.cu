@@ -1913,7 +1913,9 @@ int resident_clusters(const Variant& v) {
 // a warm-up run, then one timed run of the captured program.
 double time_candidate(ss_engine* e, const ss_run_config& c, uint64_t first, int64_t sample,
                       int precision, const Variant& v) {
-  sample = std::max<int64_t>(sample, 4 * static_cast<int64_t>(resident_clusters(v)));
+  // a split cluster carries one of a realisation's two vectors
+  const int64_t per_wave = resident_clusters(v) / (v.split ? 2 : 1);
+  sample = std::max<int64_t>(sample, 4 * std::max<int64_t>(per_wave, 1));
   ss_batch* b = nullptr;
   g_force = &v;
   const int rc = ss_batch_create(e, &c, first, sample, precision, &b);
