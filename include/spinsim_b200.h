@@ -137,8 +137,10 @@ typedef struct ss_run_config {
   int32_t spin_choices[8];
   /* additive: in SS_PRECISION_MIXED, a realisation whose Chebyshev orders
      per state vector exceed this runs in the FP64 kernel of the same batch
-     (FP32 coefficient rounding grows with the order count); 0 = 40000,
-     negative = never.  Sizes without an FP64 kernel stay mixed. */
+     (FP32 coefficient rounding grows with the order count); 0 = 40000
+     for L <= 15 with L = 16 staying mixed (its FP64 kernel takes the heavy
+     tail one 16-CTA cluster each), > 0 = that limit at every size,
+     negative = never. */
   int64_t mixed_order_limit;
   /* additive: a parameter sweep for the batched engine.  With
      sweep_points = P > 0 a batch of `count` realisations is P consecutive

@@ -941,6 +941,9 @@ const std::vector<Variant>& variants() {
       // clusters of their own
       make_dist_variant<14, 4, 1, float, true>(), make_dist_variant<15, 4, 2, float, true>(),
       make_dist_variant<16, 4, 3, float, true>(),
+      // FP64 at L = 16: 16 CTAs per vector (Ll = 12, the FP64 L = 13..15
+      // layout), which only the split form fits in one cluster
+      make_dist_variant<16, 3, 4, double, true>(),
   };
   return v;
 }
@@ -1229,14 +1232,21 @@ void exact_transverse(int L, const double* f, int mode, double tau, Expansion& e
 }
 
 constexpr int64_t kDefaultMixedOrderLimit = 40000;
+// Largest size the default limit routes.  L = 16's FP64 kernel (16-CTA split
+// clusters) takes its heaviest realisations one cluster each: on B200 routing
+// them halves the size's batch rate, while mixed runs stay within 3e-7 of
+// FP64 in the correlation over ~5e5 orders per state at L = 16.
+constexpr int kDefaultRouteMaxL = 15;
 
 // Mixed precision stores every coefficient as one FP32 number; the rounding
 // is a fixed perturbation of the Hamiltonian whose effect on the echo grows
 // with the number of orders applied.  A realisation past `limit` orders per
-// state vector therefore runs in FP64 (when its size has an FP64 kernel).
+// state vector therefore runs in FP64 (when its size has an FP64 kernel; with
+// the default limit, up to kDefaultRouteMaxL).
 bool stays_mixed(const ss_run_config& c, int L, int64_t orders_per_state) {
   const int64_t limit = c.mixed_order_limit == 0 ? kDefaultMixedOrderLimit : c.mixed_order_limit;
   if (limit < 0 || orders_per_state <= limit) return true;
+  if (c.mixed_order_limit == 0 && L > kDefaultRouteMaxL) return true;
   return find_variant(L, false) == nullptr;
 }
 
@@ -1460,8 +1470,7 @@ void build_plan(ss_batch* b, const ss_run_config& c) {
     measured.push_back(ns);
     if (!bk.var) {
       fail(SS_ERR_INVALID_ARGUMENT,
-           std::string("the batched engine covers L = 6..") + (mixed ? "16" : "15") +
-               " in this precision; got L = " + std::to_string(L));
+           "the batched engine covers L = 6..16; got L = " + std::to_string(L));
     }
     // Split clusters keep both vectors of every realisation of a launch at
     // every measurement point; the bucket runs in launches of `chunk`
@@ -1470,10 +1479,11 @@ void build_plan(ss_batch* b, const ss_run_config& c) {
     if (bk.var->split) {
       const size_t per_slot = b->times.size() * 2 * (size_t{1} << L) * sizeof(double2);
       const size_t fit = per_slot > 0 ? static_cast<size_t>(g_snap_budget.load()) / per_slot : list.size();
-      if (fit < std::min(list.size(), kSnapMinSlots)) {
-        bk.var = find_variant(L, mixed);
-      } else {
-        bk.chunk = static_cast<int>(std::min(fit, list.size()));
+      const Variant* paired = find_variant(L, mixed);
+      if (fit < std::min(list.size(), kSnapMinSlots) && !paired->split) {
+        bk.var = paired;
+      } else {  // a size whose only schedule is split runs at least one per launch
+        bk.chunk = static_cast<int>(std::max<size_t>(1, std::min(fit, list.size())));
       }
     }
     // The paired cluster kernel's measurement keeps one partial sum per

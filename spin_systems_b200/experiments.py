@@ -125,6 +125,7 @@ def long_run(args) -> dict:
     every = args.every
     spec = workloads.long_propagation(nspins=L, steps=args.steps, dt=0.1, every=every,
                                       epsilon=args.epsilon)
+    spec.mixed_order_limit = -1  # the mixed run stays mixed at every order count
     cfg = spec.config()
     points = spec.measurement_count()
     width = spec.width()

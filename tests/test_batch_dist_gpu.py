@@ -1,5 +1,5 @@
 """Batched sizes whose vectors are spread over a thread-block cluster
-(k_batch_dist: L = 13..15 in FP64, 14..16 mixed), against the C port of the
+(k_batch_dist: L = 13..16 in FP64, 14..16 mixed), against the C port of the
 reference on fresh realisations.  Same bars as the one-CTA sizes: FP64 to
 1e-10, mixed precision to 1e-6 in echo error.  The short program puts
 transverse fields, ideal pulses, every observable (a magnetisation on a
@@ -43,12 +43,14 @@ def corr0(cfg, count, L):
     return np.array(out)
 
 
-@pytest.mark.parametrize("L", [13, 14, 15])
+@pytest.mark.parametrize("L", [13, 14, 15, 16])
 def test_fp64_cluster_sizes_match_the_oracle(engine, port, L):
-    spec = short_spec(L, 2)
+    # L = 16 runs on split clusters of 16 CTAs (its only FP64 schedule)
+    n = 2 if L < 16 else 1
+    spec = short_spec(L, n)
     cfg = spec.config()
-    want = np.stack([port.run_realization(cfg, i)[1] for i in range(2)])
-    b = ss.Batch(engine, cfg, 0, 2, abi.FP64)
+    want = np.stack([port.run_realization(cfg, i)[1] for i in range(n)])
+    b = ss.Batch(engine, cfg, 0, n, abi.FP64)
     assert (b.precisions() == abi.FP64).all()
     _, rows = b.run()
     assert np.abs(rows - want).max() < 1e-10

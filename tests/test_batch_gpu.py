@@ -146,7 +146,9 @@ def test_mixed_order_limit_switches(engine):
     spec.mixed_order_limit = -1
     assert (ss.Batch(engine, spec.config(), 0, 6, abi.MIXED).precisions() == abi.MIXED).all()
     spec16 = workloads.xy8_finite(nspins=16, realizations=2, blocks=1)
-    spec16.mixed_order_limit = 1  # no FP64 kernel at L = 16: stays mixed
+    spec16.mixed_order_limit = 1  # an explicit limit routes L = 16 to its FP64 kernel
+    assert (ss.Batch(engine, spec16.config(), 0, 2, abi.MIXED).precisions() == abi.FP64).all()
+    spec16.mixed_order_limit = 0  # the default keeps L = 16 mixed
     assert (ss.Batch(engine, spec16.config(), 0, 2, abi.MIXED).precisions() == abi.MIXED).all()
     assert (ss.Batch(engine, spec.config(), 0, 6, abi.FP64).precisions() == abi.FP64).all()
 

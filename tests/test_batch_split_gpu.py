@@ -95,3 +95,21 @@ def test_split_schedule_in_launches_of_the_snapshot_budget(engine, tmp_path):
     assert launches(one) == 3 and launches(two) == 5 and launches(paired) == 2
     assert np.array_equal(rows_one, rows_two)
     assert np.abs(rows_paired - rows_one).max() <= 1e-6 * max(1.0, np.abs(rows_one).max())
+
+
+def test_fp64_l16_has_only_split_clusters_and_runs_one_per_launch_when_tight(engine):
+    # FP64 at L = 16 has no paired schedule: a budget below one realisation's
+    # snapshots still runs, one realisation per launch, with the same rows.
+    cfg = short_spec(16, 2).config()
+    ss.clear_schedule()
+    b = ss.Batch(engine, cfg, 0, 2, abi.FP64)
+    _, rows = b.run()
+    assert launches(b) == 3
+    ss.set_snapshot_budget(1)
+    try:
+        tight = ss.Batch(engine, cfg, 0, 2, abi.FP64)
+        _, rows_tight = tight.run()
+    finally:
+        ss.set_snapshot_budget(16 << 30)
+    assert launches(tight) == 5  # prepare + two (kernel, measurement) pairs
+    assert np.array_equal(rows, rows_tight)

@@ -10,14 +10,14 @@ def test_every_size_has_a_default_and_the_alternatives_are_listed():
     assert len(names) == len(set(names))
     sizes_mixed = {int(n.split(".")[0][1:]) for n in names if ".f32." in n}
     sizes_fp64 = {int(n.split(".")[0][1:]) for n in names if ".f64." in n}
-    assert sizes_mixed == set(range(6, 17)) and sizes_fp64 == set(range(6, 16))
+    assert sizes_mixed == set(range(6, 17)) and sizes_fp64 == set(range(6, 17))
     # sizes with a choice to make
     for L in (10, 11, 12, 13, 14, 15, 16):
         assert sum(n.startswith(f"L{L}.") and ".f32." in n for n in names) >= 2
     assert "L16.R4.f32.global.c8" in names
     # state and reference on clusters of their own at the cluster sizes
     assert {"L14.R4.f32.global.c2.split", "L15.R4.f32.global.c4.split",
-            "L16.R4.f32.global.c8.split"} <= set(names)
+            "L16.R4.f32.global.c8.split", "L16.R3.f64.global.c16.split"} <= set(names)
     for name, threads, smem in ss.variants():
         assert 32 <= threads <= 1024 and smem <= 232448
 
