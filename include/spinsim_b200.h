@@ -364,7 +364,9 @@ int ss_batch_variants(char* buf, size_t cap, size_t* needed);
  * at every measurement point; a bucket runs in launches whose snapshots fit
  * `bytes` of device memory (default 16 GiB), or with the paired schedule of
  * its size when fewer than 64 realisations (or the whole bucket) would fit.
- * Process-wide; applies to batches created afterwards.  bytes >= 0. */
+ * A size with no paired schedule (FP64 at L = 16) runs at least one
+ * realisation per launch.  Process-wide; applies to batches created
+ * afterwards.  bytes >= 0. */
 int ss_set_snapshot_budget(int64_t bytes);
 
 /* -------------------------------------------------------- echo surrogate
