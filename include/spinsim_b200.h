@@ -341,7 +341,8 @@ int ss_batch_precisions(const ss_batch* batch, int32_t* precision,
  * Each batched size has candidate schedules -- register bits per thread
  * (the term grouping of the layout passes) and CTAs per state vector.
  * ss_batch_tune times every candidate of every size the config can draw
- * (and, for SS_PRECISION_MIXED, the FP64 routing kernels) on realisations
+ * (and, for SS_PRECISION_MIXED, the FP64 kernels of the sizes whose
+ * realisations mixed_order_limit can route) on realisations
  * from `first` of the config's own program -- `sample` of them, raised to
  * four waves of the candidate's resident clusters -- installs the
  * fastest in the process-wide schedule table keyed by device name, size and

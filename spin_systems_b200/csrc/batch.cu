@@ -10,6 +10,7 @@
 #include <atomic>
 #include <cmath>
 #include <fstream>
+#include <limits>
 #include <map>
 #include <mutex>
 #include <sstream>
@@ -1984,6 +1985,11 @@ int ss_batch_tune(ss_engine* e, const ss_run_config* config, uint64_t first, int
     if (precision == SS_PRECISION_MIXED) precs.push_back(SS_PRECISION_FP64);  // routing target
     for (int L : sizes) {
       for (int prec : precs) {
+        // FP64 as the routing target only where this config's mixed
+        // realisations of size L can be routed at all
+        if (prec != precision && stays_mixed(*config, L, std::numeric_limits<int64_t>::max())) {
+          continue;
+        }
         const bool mixed = prec == SS_PRECISION_MIXED;
         ss_run_config c = *config;
         c.n_spin_choices = 1;  // every sampled realisation has L spins (the

@@ -33,6 +33,20 @@ def test_tuner_fills_the_table_and_writes_the_cache(engine, tmp_path):
         (r["L"], r["precision"], r["variant"]) for r in rows}
 
 
+def test_tuner_times_fp64_only_where_mixed_realisations_can_route(engine):
+    # The default limit keeps L = 16 mixed, so a mixed tune there installs
+    # no FP64 schedule; an explicit limit routes L = 16 and tunes its FP64
+    # (split-cluster) kernel as well.
+    spec = _spec()
+    spec.spin_choices = (16,)
+    for limit, want in ((0, {"mixed"}), (40000, {"mixed", "fp64"})):
+        ss.clear_schedule()
+        spec.mixed_order_limit = limit
+        rows = ss.tune(engine, spec.config(), 0, 4, abi.MIXED)
+        assert {r["precision"] for r in rows if r["L"] == 16} == want
+    ss.clear_schedule()
+
+
 @pytest.mark.parametrize("variant", ["L10.R3.f32.smem.c1", "L11.R3.f32.smem.c1",
                                      "L12.R3.f32.smem.c1", "L13.R4.f32.global.c2",
                                      "L11.R4.f64.smem.c1", "L12.R3.f64.global.c2",
