@@ -52,6 +52,15 @@ enum ss_precision {
   SS_PRECISION_FP64 = 0,  /* everything in FP64                                */
   SS_PRECISION_MIXED = 1  /* FP32 T_n recursion, FP64 series sum and reductions */
 };
+/* Kernel family of the plain propagator's Chebyshev order. */
+enum ss_evolve_kernel {
+  SS_KERNEL_AUTO = 0,        /* the faster family for the vector's size          */
+  SS_KERNEL_GATHER = 1,      /* one sweep per order; every amplitude gathers its
+                                partners through L1                              */
+  SS_KERNEL_TILED = 2,       /* a few passes per order over shared-memory tiles
+                                of 12 spins (FP64) or 13 (mixed): needs L >= that */
+  SS_KERNEL_TILED_SMALL = 3  /* the same with tiles of 8 spins (L >= 8)          */
+};
 
 enum ss_initial_state {
   SS_INIT_RANDOM = 0,         /* core: InitialStateKind::Random (Ensemble.hpp:21-26) */
@@ -257,6 +266,24 @@ int ss_evolve(const ss_ham* ham, ss_state* psi, const double* coeffs,
 int ss_propagate(const ss_ham* ham, ss_state* psi, int mode, double tau,
                  int64_t nsteps, int autonormalize, double epsilon,
                  int64_t* order_used);
+/* The same two calls with a precision (ss_precision) and a kernel family
+ * (ss_evolve_kernel).  The reference propagates in FP64 only
+ * (src/core/Propagator.cpp:46-100); SS_PRECISION_MIXED keeps psi, the series
+ * weights, the diagonal and each T_n's formation in FP64 and stores the
+ * Chebyshev vectors T_n and the off-diagonal partial sums in FP32.
+ * ss_evolve / ss_propagate are these with SS_PRECISION_FP64, SS_KERNEL_AUTO. */
+int ss_evolve_ex(const ss_ham* ham, ss_state* psi, const double* coeffs,
+                 int64_t ncoeffs, double bound, int mode, int64_t nsteps,
+                 int autonormalize, int precision, int kernel);
+int ss_propagate_ex(const ss_ham* ham, ss_state* psi, int mode, double tau,
+                    int64_t nsteps, int autonormalize, double epsilon,
+                    int precision, int kernel, int64_t* order_used);
+/* Host only, no counterpart in the reference: the tile patterns of
+ * SS_KERNEL_TILED for an nspins-spin vector and tiles of tile_bits spins,
+ * one bit mask per pass (every pair of spins shares a pattern; the last pass
+ * forms T_n).  *npass receives the count; masks (capacity cap) may be NULL. */
+int ss_tile_plan(int nspins, int tile_bits, int32_t* npass, uint32_t* masks,
+                 int32_t cap);
 
 /* ------------------------------------------------------------ gates
  * src/core/Gate.cpp:20-33 Rotation2x2::make; :60-85 SpinRotation::apply;
@@ -303,6 +330,12 @@ int ss_realization_setup(const ss_run_config* config, uint64_t index,
  * times: points; values: points x width (see ss_batch_shape). */
 int ss_run_realization(ss_engine* engine, const ss_run_config* config,
                        uint64_t index, double* times, double* values);
+/* The same with the propagator's precision (ss_precision) and kernel family
+ * (ss_evolve_kernel), as ss_propagate_ex takes them; ss_run_realization is
+ * this with SS_PRECISION_FP64 and SS_KERNEL_AUTO. */
+int ss_run_realization_ex(ss_engine* engine, const ss_run_config* config,
+                          uint64_t index, int precision, int kernel,
+                          double* times, double* values);
 
 /* -------------------------------------------------------- batched engine
  * Runs `count` realisations (indices first..first+count-1) of a whole

@@ -88,6 +88,12 @@ def load(path: Path = LIB_PATH) -> C.CDLL:
                               C.c_int64, C.c_int]
     lib.ss_propagate.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_int64, C.c_int,
                                  C.c_double, C.POINTER(C.c_int64)]
+    lib.ss_evolve_ex.argtypes = [C.c_void_p, C.c_void_p, _dp, C.c_int64, C.c_double, C.c_int,
+                                 C.c_int64, C.c_int, C.c_int, C.c_int]
+    lib.ss_propagate_ex.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_int64,
+                                    C.c_int, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_int64)]
+    lib.ss_tile_plan.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_uint32),
+                                 C.c_int32]
     lib.ss_bessel.argtypes = [C.c_int, C.c_double, C.c_int64, _dp, C.POINTER(C.c_int64)]
     lib.ss_chebyshev_build.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_int64, _dp,
                                        C.c_int64, C.POINTER(C.c_int64), _dp]
@@ -98,6 +104,8 @@ def load(path: Path = LIB_PATH) -> C.CDLL:
     lib.ss_batch_create.argtypes = [C.c_void_p, C.POINTER(SsRunConfig), C.c_uint64, C.c_int64,
                                     C.c_int, C.POINTER(C.c_void_p)]
     lib.ss_run_realization.argtypes = [C.c_void_p, C.POINTER(SsRunConfig), C.c_uint64, _dp, _dp]
+    lib.ss_run_realization_ex.argtypes = [C.c_void_p, C.POINTER(SsRunConfig), C.c_uint64, C.c_int,
+                                          C.c_int, _dp, _dp]
     lib.ss_measure_corr_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p,
                                             _dp]
     _lib = lib
@@ -334,12 +342,17 @@ def chebyshev(mode: int, bound: float, tau: float, epsilon: float, max_order: in
 
 
 class Propagator:
-    """Propagator::evolve (src/core/Propagator.cpp:75-100) on the device."""
+    """Propagator::evolve (src/core/Propagator.cpp:75-100) on the device.
 
-    def __init__(self, nspins: int, epsilon: float = 1e-7):
+    ``precision`` (abi.FP64 / abi.MIXED) and ``kernel`` (abi.KERNEL_*) choose
+    the arithmetic and the order kernel; the defaults are the reference's FP64
+    and the faster kernel family for the size."""
+
+    def __init__(self, nspins: int, epsilon: float = 1e-7, precision: int = 0, kernel: int = 0):
         if not epsilon > 0:
             raise InvalidArgumentError(1, "epsilon must be positive")
         self.nspins, self.epsilon, self.last_order = nspins, epsilon, 0
+        self.precision, self.kernel = precision, kernel
 
     def evolve(self, ham: Hamiltonian, mode: int, psi: StateVector, tau: float, nsteps: int,
                autonormalize: bool = False) -> None:
@@ -348,10 +361,22 @@ class Propagator:
         if psi.nspins != self.nspins:
             raise InvalidArgumentError(1, "state does not match the propagator's size")
         order = C.c_int64(0)
-        check(ham.lib.ss_propagate(ham.handle, psi.handle, mode, tau, nsteps, int(autonormalize),
-                                   self.epsilon, C.byref(order)))
+        check(ham.lib.ss_propagate_ex(ham.handle, psi.handle, mode, tau, nsteps,
+                                      int(autonormalize), self.epsilon, self.precision,
+                                      self.kernel, C.byref(order)))
         if nsteps:
             self.last_order = order.value
+
+
+def tile_plan(nspins: int, tile_bits: int) -> list:
+    """The tiled kernel's tile patterns (bit masks, one per pass; the last
+    forms T_n) for an nspins-spin vector and tiles of tile_bits spins."""
+    lib = load()
+    n = C.c_int32()
+    check(lib.ss_tile_plan(nspins, tile_bits, C.byref(n), None, 0))
+    masks = (C.c_uint32 * max(1, n.value))()
+    check(lib.ss_tile_plan(nspins, tile_bits, C.byref(n), masks, n.value))
+    return [int(m) for m in masks[: n.value]]
 
 
 def rotation_matrix(axis: Sequence[float], angle: float) -> np.ndarray:
@@ -416,11 +441,14 @@ def realization_setup(cfg: SsRunConfig, index: int, lmax: int):
                 J=J[: 3 * P].copy(), psi0=psi0[: 2 << L].copy())
 
 
-def run_realization(engine: Engine, cfg: SsRunConfig, index: int, points: int, width: int):
-    """The plain FP64 path for one realisation (ss_run_realization)."""
+def run_realization(engine: Engine, cfg: SsRunConfig, index: int, points: int, width: int,
+                    precision: int = abi.FP64, kernel: int = abi.KERNEL_AUTO):
+    """The plain path for one realisation (ss_run_realization_ex): FP64 by
+    default, or mixed precision, with the propagator's kernel family."""
     times = np.zeros(max(points, 1))
     values = np.zeros(max(points * width, 1))
-    check(engine.lib.ss_run_realization(engine.handle, C.byref(cfg), index, _d(times), _d(values)))
+    check(engine.lib.ss_run_realization_ex(engine.handle, C.byref(cfg), index, precision, kernel,
+                                           _d(times), _d(values)))
     return times[:points], values[: points * width].reshape(points, width)
 
 

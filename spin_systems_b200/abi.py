@@ -22,6 +22,7 @@ STATUS_NAMES = {
 AXIS = {"x": 0, "y": 1, "z": 2}
 REAL, IMAGINARY = 0, 1
 FP64, MIXED = 0, 1
+KERNEL_AUTO, KERNEL_GATHER, KERNEL_TILED, KERNEL_TILED_SMALL = 0, 1, 2, 3
 INIT = {"random": 0, "up": 1, "down": 2, "basis": 3, "random_product": 4}
 EVOLVE, PULSE, MEASURE, REPEAT = 0, 1, 2, 3
 OBS_CORR, OBS_MAG, OBS_NORM, OBS_ENERGY = 0, 1, 2, 3

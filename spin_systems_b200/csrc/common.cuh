@@ -48,8 +48,12 @@ struct StepGraph {
   const void* psi = nullptr;
   const void* t0 = nullptr;
   const void* t1 = nullptr;
+  const void* part = nullptr;    // tiled kernel: the partial-sum vector
+  const void* passes = nullptr;  // tiled kernel: the per-pass tables
   size_t n = 0;
   int autonormalize = 0;
+  int precision = 0;
+  int kernel = 0;
   std::vector<double> weights;
   cudaGraphExec_t exec = nullptr;
   int64_t kernels = 0;  // kernel nodes per replay
@@ -71,6 +75,8 @@ struct ss_engine {
   int* host_flags = nullptr;
   double2* evolve_t[2] = {nullptr, nullptr};  // the propagator's two work vectors
   int evolve_nspins = 0;                      // their capacity, as L
+  double2* evolve_part = nullptr;             // tiled kernel: partial sums of H T_{n-1}
+  int evolve_part_nspins = 0;
   std::vector<ss::StepGraph> step_graphs;     // the plain propagator's captured steps
   uint64_t graph_clock = 0;
   std::atomic<int64_t> launches{0};

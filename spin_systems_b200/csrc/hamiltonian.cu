@@ -3,6 +3,7 @@
 #include <cmath>
 
 #include "hamiltonian.cuh"
+#include "tiled.hpp"
 
 namespace ss {
 
@@ -142,6 +143,7 @@ int ss_ham_destroy(ss_ham* h) {
     cudaStreamSynchronize(h->engine->stream);
     cudaFree(h->diag);
     cudaFree(h->dev_terms);
+    tiled_release(h);
     delete h;
   });
 }
@@ -175,6 +177,7 @@ int ss_ham_set_terms(ss_ham* h, const double* fields, int npairs, const int32_t*
     h->pairs = std::move(list);
     h->diag_valid = false;
     h->terms_valid = false;
+    h->tiled_terms_valid = false;
   });
 }
 
@@ -185,6 +188,7 @@ int ss_ham_set_fields(ss_ham* h, const double* fields) {
     h->fields.assign(fields, fields + 3 * h->nspins);
     h->diag_valid = false;
     h->terms_valid = false;
+    h->tiled_terms_valid = false;
   });
 }
 

@@ -40,16 +40,18 @@ void build_terms(int nspins, const double* fields, const std::vector<PairTerm>& 
                  double scale, HamTerms* out);
 
 // (s*H x)[k] gathered from x's partners: the diagonal, then transverse fields,
-// then the off-diagonal channel of every coupling.
+// then the off-diagonal channel of every coupling.  x holds double2 (FP64) or
+// float2 (the mixed path's FP32 vectors) amplitudes; the sum is FP64 either way.
+template <typename C2>
 __device__ __forceinline__ double2 ham_gather(const HamTerms* __restrict__ t,
                                               const double* __restrict__ diag,
-                                              const double2* __restrict__ x, size_t k) {
-  const double2 self = x[k];
+                                              const C2* __restrict__ x, size_t k) {
+  const C2 self = x[k];
   const double g = t->scale * diag[k];
   double re = g * self.x, im = g * self.y;
   for (int i = 0; i < t->ntrans; ++i) {
     const unsigned int m = t->trans_mask[i];
-    const double2 p = x[k ^ m];
+    const C2 p = x[k ^ m];
     const double cx = t->trans_cx[i];
     const double cy = (k & m) ? -t->trans_cy[i] : t->trans_cy[i];
     re += cx * p.x - cy * p.y;
@@ -63,13 +65,15 @@ __device__ __forceinline__ double2 ham_gather(const HamTerms* __restrict__ t,
     const bool aligned = ((k & lo) != 0) == ((k & hi) != 0);
     const double c = aligned ? t->pair_fb[i] : t->pair_ff[i];
     if (c != 0.0) {
-      const double2 p = x[k ^ (lo | hi)];
+      const C2 p = x[k ^ (lo | hi)];
       re += c * p.x;
       im += c * p.y;
     }
   }
   return make_double2(re, im);
 }
+
+struct TiledTables;
 
 }  // namespace ss
 
@@ -83,6 +87,8 @@ struct ss_ham {
   ss::HamTerms* dev_terms = nullptr;     // device table for `terms_scale`
   double terms_scale = 0.0;
   bool terms_valid = false;
+  ss::TiledTables* tiled = nullptr;      // the tiled kernel's per-pass tables (tiled.cu)
+  bool tiled_terms_valid = false;        // false once fields or couplings change
   size_t size() const { return size_t{1} << nspins; }
 };
 

@@ -1,7 +1,8 @@
-// The plain FP64 path for one realisation: runRealization
-// (io/Experiment.cpp:10-55) driving Sequence::run (src/sequence/Sequence.cpp)
-// on the device, one Propagator::evolve per Evolve step for the state and again
-// for the reference, exactly the reference's call structure.
+// The plain path for one realisation: runRealization (io/Experiment.cpp:10-55)
+// driving Sequence::run (src/sequence/Sequence.cpp) on the device, one
+// Propagator::evolve per Evolve step for the state and again for the
+// reference, exactly the reference's call structure (FP64 by default; the
+// _ex entry point takes the propagator's precision and kernel family).
 #include <cmath>
 #include <memory>
 
@@ -9,8 +10,9 @@
 
 namespace ss {
 
-void evolve_fp64(ss_ham* h, ss_state* psi, const std::vector<double>& weights, double bound,
-                 int64_t nsteps, bool autonormalize);
+void evolve(ss_ham* h, ss_state* psi, const std::vector<double>& weights, double bound,
+            int64_t nsteps, bool autonormalize, int precision, int kernel);
+int resolve_kernel(int nspins, int precision, int kernel);
 void rotation_matrix(const double axis[3], double angle, double u[8]);
 void rotate(ss_state* psi, const double u[8], const int32_t* targets, int ntargets);
 void total_spin(int axis, const ss_state* in, ss_state* out);
@@ -56,6 +58,8 @@ struct Runner {
   int64_t width = 0;
   double* times;
   double* values;
+  int precision = SS_PRECISION_FP64;
+  int kernel = SS_KERNEL_AUTO;
 
   ss_ham* ham_for(int table) {
     const size_t slot = static_cast<size_t>(table + 1);
@@ -74,8 +78,8 @@ struct Runner {
                                      tau, cfg.epsilon);
       if (ex.order() > 0) {
         const std::vector<double> w = series_weights(ex, s.mode);
-        evolve_fp64(h, psi.get(), w, ex.bound, s.count, s.autonormalize != 0);
-        evolve_fp64(h, ref.get(), w, ex.bound, s.count, s.autonormalize != 0);
+        ss::evolve(h, psi.get(), w, ex.bound, s.count, s.autonormalize != 0, precision, kernel);
+        ss::evolve(h, ref.get(), w, ex.bound, s.count, s.autonormalize != 0, precision, kernel);
       }
     }
     time += tau * static_cast<double>(s.count);
@@ -183,10 +187,13 @@ void validate_config(const ss_run_config& c) {
 }
 
 void run_realization_plain(ss_engine* e, const ss_run_config& cfg, uint64_t index, double* times,
-                           double* values) {
+                           double* values, int precision, int kernel) {
   validate_config(cfg);
   Runner x{cfg, e, assemble_realization(cfg, index), {}, nullptr, nullptr};
   const int L = x.r.nspins;
+  resolve_kernel(L, precision, kernel);  // rejects unknown or too-small choices up front
+  x.precision = precision;
+  x.kernel = kernel;
   x.hams.resize(static_cast<size_t>(cfg.n_step_fields) + 1);
   x.hams[0] = make_ham(e, L, x.r.fields.data(), x.r.pairs);
   x.psi = make_state(e, L);
@@ -210,6 +217,17 @@ extern "C" int ss_run_realization(ss_engine* engine, const ss_run_config* config
   return guarded([&] {
     require(engine != nullptr && config != nullptr && times != nullptr && values != nullptr,
             SS_ERR_INVALID_ARGUMENT, "null argument");
-    run_realization_plain(engine, *config, index, times, values);
+    run_realization_plain(engine, *config, index, times, values, SS_PRECISION_FP64,
+                          SS_KERNEL_AUTO);
+  });
+}
+
+extern "C" int ss_run_realization_ex(ss_engine* engine, const ss_run_config* config,
+                                     uint64_t index, int precision, int kernel, double* times,
+                                     double* values) {
+  return guarded([&] {
+    require(engine != nullptr && config != nullptr && times != nullptr && values != nullptr,
+            SS_ERR_INVALID_ARGUMENT, "null argument");
+    run_realization_plain(engine, *config, index, times, values, precision, kernel);
   });
 }

@@ -201,6 +201,7 @@ int ss_engine_destroy(ss_engine* e) {
     cudaFree(e->dev_flags);
     cudaFree(e->evolve_t[0]);
     cudaFree(e->evolve_t[1]);
+    cudaFree(e->evolve_part);
     for (ss::StepGraph& g : e->step_graphs) {
       if (g.exec) cudaGraphExecDestroy(g.exec);
     }

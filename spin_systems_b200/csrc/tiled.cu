@@ -1,0 +1,756 @@
+// The plain propagator's order kernel for large vectors.
+//
+// The fused gather kernel (propagator.cu) reads all ~L^2/4 anti-aligned
+// partners of every amplitude one double2 at a time through L1: at L = 24
+// that is 138 partner loads per amplitude-order, and the kernel is bound by
+// their delivery.  Here one Chebyshev order is a few passes instead.  Pass p
+// owns a set S_p of B spins (a "tile" pattern, B = 12 in FP64, 13 in mixed
+// precision); the vector splits into 2^(L-B) tiles, each holding the 2^B
+// amplitudes that agree on every spin outside S_p.  A CTA copies its tile of
+// T_{n-1} into shared memory (cp.async, contiguous runs along the tile's low
+// bits), applies every coupling assigned to the pass with the batched
+// engine's register-blocked layouts (each partner block read from shared
+// memory serves up to R couplings, couplings inside a register group come
+// from registers), and accumulates the partial H T_{n-1} in a vector `part`
+// of the same layout as the state.  The patterns are a pair covering: every
+// coupling (i, j) has a pass whose tile holds both spins, so every coupling
+// is applied on chip, exactly once.  The last pass also adds the diagonal
+// (streamed, FP64) and forms T_n = 2H^ T_{n-1} - T_{n-2} and psi += c_n T_n,
+// the reference's recurrence (src/core/Propagator.cpp:58-72) and its
+// Hamiltonian (src/core/Hamiltonian.cpp:95-127) in one sweep per pass.
+//
+// DRAM traffic per amplitude-order with P passes: T_{n-1} once per pass,
+// the partial written by the first pass, read and written by the middle
+// ones, read by the last, and the last pass's diagonal, T_{n-2}, T_n and psi:
+//   FP64  (16 B amplitudes):  16 P + 32 (P - 1) + 8 + 32 + 32  = 48 P + 40 B
+//   mixed ( 8 B amplitudes):   8 P + 16 (P - 1) + 8 + 16 + 32  = 24 P + 40 B
+// against the single-sweep 80 / 56 B (+8 B of diagonal) that needs every
+// partner on chip at once.  At L = 24 P = 6 (a lower bound for tiles of
+// 12-14 spins that keep low bits for coalescing).
+//
+// Mixed precision: T vectors and the partial sums are FP32 and the couplings
+// are applied as FP32 numbers; the diagonal, T_n's formation, the series
+// weights and psi are FP64 (the batched engine's scheme).
+#include <algorithm>
+#include <map>
+#include <mutex>
+#include <utility>
+
+#include "batch_kernel.cuh"
+#include "hamiltonian.cuh"
+#include "tiled.hpp"
+
+namespace ss {
+namespace tiled {
+
+using batch::cross_block;
+using batch::Cplx;
+using batch::cz;
+using batch::Geo;
+using batch::pad;
+using batch::Padded;
+
+constexpr int kMaxTile = 13;
+constexpr int kMaxLayouts = 8;
+
+enum PassKind { PASS_FIRST = 0, PASS_MID = 1, PASS_LAST = 2, PASS_ONLY = 3 };
+
+// One pass: where the tile's spins sit in the basis index, which couplings it
+// applies (tile-local upper-triangular tables, zero where another pass owns
+// the pair), and per layout the partner blocks worth reading.
+struct PassDev {
+  uint32_t tile_pos[kMaxTile];   // basis bit of tile-local bit b
+  uint32_t outer_pos[kMaxSpins]; // basis bits of the tile index, low to high
+  int nouter;
+  int has_trans;                 // a transverse field is applied in this pass
+  int has_fb;                    // a |dd><uu| coefficient is non-zero
+  int pad_;
+  uint32_t jmask[kMaxLayouts];   // layout g: tile-local spins j with a partner block
+  uint32_t rmask[kMaxLayouts];   // layout g: register pairs (p * R + q) with a coefficient
+  double cff[kMaxTile * kMaxTile];  // [i * B + j], i < j: scale (jx + jy) / 4
+  double cfb[kMaxTile * kMaxTile];  // scale (jx - jy) / 4
+  double ccx[kMaxTile];             // scale hx / 2
+  double ccy[kMaxTile];             // scale hy / 2
+};
+
+struct OrderArgs {
+  const void* cur;      // T_{n-1}
+  void* prev;           // T_{n-2}; T_n in the last pass
+  void* part;           // partial H T_{n-1}
+  double2* psi;
+  const double* diag;   // sigma_z diagonal, unscaled
+  double dscale;        // scale of the diagonal
+  double cr, ci;        // series weight c_n
+  uint32_t ntiles;
+  int first;            // order 1: T_1 = H^ T_0
+};
+
+// ------------------------------------------------------------------ host: plan
+
+namespace {
+
+// Local search for a pair covering of spins u .. L-1 by P tiles of B - u
+// spins (spins 0 .. u-1 are in every tile).  Deterministic for a seed.
+bool search_cover(int L, int B, int u, int P, uint64_t seed, int iters,
+                  std::vector<uint32_t>* out) {
+  const int n = L - u, c = B - u;
+  if (c <= 0 || c > n) return false;
+  std::mt19937_64 rng(seed);
+  auto rnd = [&](int m) { return static_cast<int>(rng() % static_cast<uint64_t>(m)); };
+  std::vector<std::vector<int>> tiles(P);
+  std::vector<std::vector<char>> in(P, std::vector<char>(n, 0));
+  for (int t = 0; t < P; ++t) {
+    std::vector<int> all(n);
+    for (int x = 0; x < n; ++x) all[x] = x;
+    for (int x = 0; x < c; ++x) std::swap(all[x], all[x + rnd(n - x)]);
+    tiles[t].assign(all.begin(), all.begin() + c);
+    for (int x : tiles[t]) in[t][x] = 1;
+  }
+  std::vector<int> cnt(static_cast<size_t>(n) * n, 0);
+  for (int t = 0; t < P; ++t) {
+    for (int a = 0; a < c; ++a) {
+      for (int b = a + 1; b < c; ++b) {
+        ++cnt[tiles[t][a] * n + tiles[t][b]];
+        ++cnt[tiles[t][b] * n + tiles[t][a]];
+      }
+    }
+  }
+  int uncovered = 0;
+  for (int a = 0; a < n; ++a) {
+    for (int b = a + 1; b < n; ++b) uncovered += cnt[a * n + b] == 0;
+  }
+  for (int it = 0; it < iters && uncovered > 0; ++it) {
+    const int t = rnd(P), slot = rnd(c);
+    const int gone = tiles[t][slot];
+    int come = rnd(n - c);
+    for (int x = 0; x < n; ++x) {  // the come-th spin outside the tile
+      if (!in[t][x] && come-- == 0) {
+        come = x;
+        break;
+      }
+    }
+    int delta = 0;
+    for (int y : tiles[t]) {
+      if (y == gone) continue;
+      delta += cnt[gone * n + y] == 1;
+      delta -= cnt[come * n + y] == 0;
+    }
+    if (delta > 0 && rng() % 64 != 0) continue;
+    for (int y : tiles[t]) {
+      if (y == gone) continue;
+      --cnt[gone * n + y];
+      --cnt[y * n + gone];
+      ++cnt[come * n + y];
+      ++cnt[y * n + come];
+    }
+    tiles[t][slot] = come;
+    in[t][gone] = 0;
+    in[t][come] = 1;
+    uncovered += delta;
+  }
+  if (uncovered != 0) return false;
+  out->clear();
+  for (int t = 0; t < P; ++t) {
+    uint32_t m = (1u << u) - 1u;
+    for (int x : tiles[t]) m |= 1u << (u + x);
+    out->push_back(m);
+  }
+  return true;
+}
+
+// Always available: the free spins in m groups of at most (B - u) / 2, one
+// tile per pair of groups.
+std::vector<uint32_t> group_cover(int L, int B, int u) {
+  const int n = L - u, c = B - u;
+  const uint32_t low = (1u << u) - 1u;
+  if (n <= c) return {low | (((1u << n) - 1u) << u)};
+  int m = 2;
+  while ((n + m - 1) / m * 2 > c) ++m;
+  std::vector<uint32_t> groups(m, 0);
+  for (int x = 0; x < n; ++x) groups[x * m / n] |= 1u << (u + x);
+  std::vector<uint32_t> out;
+  for (int a = 0; a < m; ++a) {
+    for (int b = a + 1; b < m; ++b) out.push_back(low | groups[a] | groups[b]);
+  }
+  return out;
+}
+
+bool covers(int L, const std::vector<uint32_t>& tiles) {
+  for (int i = 0; i < L; ++i) {
+    for (int j = i + 1; j < L; ++j) {
+      const uint32_t m = (1u << i) | (1u << j);
+      if (std::none_of(tiles.begin(), tiles.end(), [m](uint32_t t) { return (t & m) == m; })) {
+        return false;
+      }
+    }
+  }
+  return true;
+}
+
+int low_run(uint32_t m) {
+  int r = 0;
+  while (r < 32 && ((m >> r) & 1u)) ++r;
+  return r;
+}
+
+std::vector<uint32_t> make_plan(int L, int B) {
+  if (L <= B) return {L >= 32 ? ~0u : (1u << L) - 1u};
+  std::vector<uint32_t> best = group_cover(L, B, 0);
+  int best_u = 0;
+  // Prefer fewer passes, then more low bits in every tile (longer contiguous
+  // runs per copy).
+  for (int u = std::min(3, B - 2); u >= 0; --u) {
+    const int n = L - u, c = B - u;
+    std::vector<uint32_t> g = group_cover(L, B, u);
+    if (g.size() < best.size() || (g.size() == best.size() && u > best_u)) {
+      best = g;
+      best_u = u;
+    }
+    const int r = (n - 1 + c - 2) / (c - 1);  // tiles per spin, at least
+    const int lb = std::max(2, (n * r + c - 1) / c);
+    for (int P = lb; P < static_cast<int>(best.size()) ||
+                     (P == static_cast<int>(best.size()) && u > best_u);
+         ++P) {
+      std::vector<uint32_t> found;
+      bool ok = false;
+      for (uint64_t seed = 1; seed <= 8 && !ok; ++seed) {
+        ok = search_cover(L, B, u, P, seed * 0x9E3779B97F4A7C15ULL + uint64_t(L * 64 + B),
+                          60000, &found);
+      }
+      if (ok) {
+        best = found;
+        best_u = u;
+        break;
+      }
+    }
+  }
+  // The kernel's tiles hold exactly B spins: top up smaller ones with the
+  // lowest spins they lack (longer contiguous runs).
+  for (uint32_t& m : best) {
+    for (int s = 0; s < L && __builtin_popcount(m) < B; ++s) m |= 1u << s;
+  }
+  // The pass that forms T_n streams psi, T_{n-2} and the diagonal: give it
+  // the longest contiguous run.
+  auto last = std::max_element(best.begin(), best.end(),
+                               [](uint32_t a, uint32_t b) { return low_run(a) < low_run(b); });
+  std::iter_swap(last, best.end() - 1);
+  return best;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------- device side
+
+__device__ __forceinline__ uint32_t deposit(uint32_t x, const uint32_t* pos, int n) {
+  uint32_t r = 0;
+  for (int b = 0; b < n; ++b) r |= ((x >> b) & 1u) << pos[b];
+  return r;
+}
+
+template <typename C2>
+__device__ __forceinline__ void cp_async(C2* dst, const C2* src) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  if constexpr (sizeof(C2) == 16) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(src) : "memory");
+  } else {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(src) : "memory");
+  }
+}
+
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+template <typename Real, int B, int R>
+struct Tile {
+  using Gm = Geo<B, R>;
+  using C2 = typename Cplx<Real>::T;
+  static constexpr int NT = Gm::NT, NA = Gm::NA, G = Gm::G;
+  static constexpr uint32_t NP = Padded<B, R>::N;
+  static constexpr size_t kSmem =
+      2 * NP * sizeof(C2) + (2 * B * B + 2 * B) * sizeof(Real) + 2 * NA * sizeof(uint32_t);
+  static_assert(G <= kMaxLayouts && B <= kMaxTile, "tile too wide");
+};
+
+// Shared-memory view of one CTA.
+template <typename Real>
+struct TileSmem {
+  using C2 = typename Cplx<Real>::T;
+  C2* buf;        // T_{n-1} tile
+  C2* acc;        // partial sums between layouts
+  const Real* cff;
+  const Real* cfb;
+  const Real* ccx;
+  const Real* ccy;
+};
+
+// One register-blocked layout over the tile (the batched engine's
+// layout_pass, restricted to the pass's couplings): own[] receives the
+// thread's T_{n-1} amplitudes, acc[] the partial sums (from shared memory, or
+// zero for the first layout of a first pass).
+template <typename Real, int B, int R, int g, bool ACC_IN>
+__device__ __forceinline__ void tile_layout(const TileSmem<Real>& sm,
+                                            typename Cplx<Real>::T (&acc)[Geo<B, R>::NA],
+                                            typename Cplx<Real>::T (&own)[Geo<B, R>::NA],
+                                            uint32_t t, uint32_t jmask, uint32_t rmask,
+                                            bool has_trans, bool has_fb) {
+  using Gm = Geo<B, R>;
+  using C2 = typename Cplx<Real>::T;
+  constexpr int b = Gm::base(g);
+  constexpr int NA = Gm::NA;
+  const uint32_t kb = ((t >> b) << (b + R)) | (t & ((1u << b) - 1u));
+  const C2* mine = sm.buf + pad<R>(kb);
+#pragma unroll
+  for (int a = 0; a < NA; ++a) own[a] = mine[pad<R>(uint32_t(a) << b)];
+  if constexpr (ACC_IN) {
+    const C2* pp = sm.acc + pad<R>(kb);
+#pragma unroll
+    for (int a = 0; a < NA; ++a) acc[a] = pp[pad<R>(uint32_t(a) << b)];
+  } else {
+#pragma unroll
+    for (int a = 0; a < NA; ++a) acc[a] = cz<C2>();
+  }
+
+  // Couplings with both spins in this register group.
+#pragma unroll
+  for (int p = 0; p < R; ++p) {
+#pragma unroll
+    for (int q = p + 1; q < R; ++q) {
+      if (Gm::pair_layout(b + p, b + q) == g && ((rmask >> (p * R + q)) & 1u)) {
+        const Real ff = sm.cff[(b + p) * B + (b + q)];
+        const Real fb = sm.cfb[(b + p) * B + (b + q)];
+#pragma unroll
+        for (int a = 0; a < NA; ++a) {
+          const int src = a ^ (1 << p) ^ (1 << q);
+          if (((a >> p) & 1) != ((a >> q) & 1)) {
+            acc[a].x += ff * own[src].x;
+            acc[a].y += ff * own[src].y;
+          } else if (has_fb) {
+            acc[a].x += fb * own[src].x;
+            acc[a].y += fb * own[src].y;
+          }
+        }
+      }
+    }
+  }
+
+  // Transverse fields assigned to this pass, on this group's spins.
+  if (has_trans) {
+#pragma unroll
+    for (int p = 0; p < R; ++p) {
+      if (Gm::first_layout(b + p) == g) {
+        const Real cx = sm.ccx[b + p], cy = sm.ccy[b + p];
+        if (cx != Real(0) || cy != Real(0)) {
+#pragma unroll
+          for (int a = 0; a < NA; ++a) {
+            const C2 v = own[a ^ (1 << p)];
+            const Real sy = ((a >> p) & 1) ? -cy : cy;
+            acc[a].x += cx * v.x - sy * v.y;
+            acc[a].y += cx * v.y + sy * v.x;
+          }
+        }
+      }
+    }
+  }
+
+  // Couplings (b + p, j) with j above the group, one partner block per j
+  // that has a coupling in this pass.
+#pragma unroll 1
+  while (jmask != 0u) {
+    const int j = __ffs(jmask) - 1;
+    jmask &= jmask - 1u;
+    const uint32_t m = 1u << j;
+    const bool bj = (kb & m) != 0;
+    Real c0[R], c1[R];
+#pragma unroll
+    for (int p = 0; p < R; ++p) {
+      const bool mine_p = Gm::cross_mine(g, p);
+      const Real ff = mine_p ? sm.cff[(b + p) * B + j] : Real(0);
+      const Real fb = mine_p ? sm.cfb[(b + p) * B + j] : Real(0);
+      c0[p] = bj ? ff : fb;
+      c1[p] = bj ? fb : ff;
+    }
+    cross_block<R, b>(acc, sm.buf + pad<R>(kb ^ m), c0, c1, bj, has_fb);
+  }
+}
+
+template <typename Real, int B, int R, int g, bool ACC0>
+__device__ __forceinline__ void tile_front(const TileSmem<Real>& sm, const PassDev* pd, uint32_t t,
+                                           bool has_trans, bool has_fb) {
+  using Gm = Geo<B, R>;
+  if constexpr (g < Gm::G - 1) {
+    using C2 = typename Cplx<Real>::T;
+    C2 acc[Gm::NA], own[Gm::NA];
+    tile_layout<Real, B, R, g, (g > 0 || ACC0)>(sm, acc, own, t, pd->jmask[g], pd->rmask[g],
+                                                 has_trans, has_fb);
+    constexpr int b = Gm::base(g);
+    const uint32_t kb = ((t >> b) << (b + R)) | (t & ((1u << b) - 1u));
+    C2* pp = sm.acc + pad<R>(kb);
+#pragma unroll
+    for (int a = 0; a < Gm::NA; ++a) pp[pad<R>(uint32_t(a) << b)] = acc[a];
+    __syncthreads();
+    tile_front<Real, B, R, g + 1, ACC0>(sm, pd, t, has_trans, has_fb);
+  }
+}
+
+// One pass of one Chebyshev order over every tile (persistent CTAs).
+template <typename Real, int B, int R, int KIND>
+__global__ void __launch_bounds__(Geo<B, R>::NT, 1)
+    k_tile(const PassDev* __restrict__ pd, OrderArgs a) {
+  using T = Tile<Real, B, R>;
+  using C2 = typename T::C2;
+  constexpr int NT = T::NT, NA = T::NA, G = T::G;
+  constexpr uint32_t NP = T::NP;
+  constexpr int bl = Geo<B, R>::base(G - 1);
+  constexpr bool kAccIn = KIND == PASS_MID || KIND == PASS_LAST;
+
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C2* buf = reinterpret_cast<C2*>(smem_raw);
+  C2* accb = buf + NP;
+  Real* cff = reinterpret_cast<Real*>(accb + NP);
+  Real* cfb = cff + B * B;
+  Real* ccx = cfb + B * B;
+  Real* ccy = ccx + B;
+  uint32_t* dep_ld = reinterpret_cast<uint32_t*>(ccy + B);
+  uint32_t* dep_rg = dep_ld + NA;
+
+  const uint32_t t = threadIdx.x;
+  for (int i = t; i < B * B; i += NT) {
+    cff[i] = Real(pd->cff[i]);
+    cfb[i] = Real(pd->cfb[i]);
+  }
+  if (t < B) {
+    ccx[t] = Real(pd->ccx[t]);
+    ccy[t] = Real(pd->ccy[t]);
+  }
+  if (t < NA) {
+    dep_ld[t] = deposit(t << (B - R), pd->tile_pos, B);
+    dep_rg[t] = deposit(t << bl, pd->tile_pos, B);
+  }
+  // Copies: thread t moves tile elements t + m NT, m < NA (consecutive lanes
+  // on consecutive tile-local indices, i.e. along the tile's low bits).
+  const uint32_t dep_t = deposit(t, pd->tile_pos, B - R);
+  const uint32_t kb_last = ((t >> bl) << (bl + R)) | (t & ((1u << bl) - 1u));
+  const uint32_t dep_kb = deposit(kb_last, pd->tile_pos, B);
+  const bool has_trans = pd->has_trans != 0, has_fb = pd->has_fb != 0;
+  const TileSmem<Real> sm{buf, accb, cff, cfb, ccx, ccy};
+  __syncthreads();
+
+  const C2* cur = static_cast<const C2*>(a.cur);
+  C2* part = static_cast<C2*>(a.part);
+  C2* prev = static_cast<C2*>(a.prev);
+  for (uint32_t tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
+    const uint32_t base = deposit(tile, pd->outer_pos, pd->nouter);
+#pragma unroll
+    for (int m = 0; m < NA; ++m) {
+      const uint32_t s = t + uint32_t(m) * NT;
+      const size_t gi = base | dep_t | dep_ld[m];
+      cp_async(buf + pad<R>(s), cur + gi);
+      if constexpr (kAccIn) cp_async(accb + pad<R>(s), part + gi);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+
+    tile_front<Real, B, R, 0, kAccIn>(sm, pd, t, has_trans, has_fb);
+    C2 acc[NA], own[NA];
+    tile_layout<Real, B, R, G - 1, true>(sm, acc, own, t, pd->jmask[G - 1], pd->rmask[G - 1],
+                                         has_trans, has_fb);
+    const size_t g0 = base | dep_kb;
+    if constexpr (KIND == PASS_FIRST || KIND == PASS_MID) {
+#pragma unroll
+      for (int x = 0; x < NA; ++x) part[g0 | dep_rg[x]] = acc[x];
+    } else {
+      const double ds = a.dscale, cr = a.cr, ci = a.ci;
+#pragma unroll
+      for (int x = 0; x < NA; ++x) {
+        const size_t gi = g0 | dep_rg[x];
+        const double d = ds * __ldg(&a.diag[gi]);
+        double hx = double(acc[x].x) + d * double(own[x].x);
+        double hy = double(acc[x].y) + d * double(own[x].y);
+        if (a.first) {
+          hx *= 0.5;
+          hy *= 0.5;
+        } else {
+          const C2 q = prev[gi];
+          hx -= double(q.x);
+          hy -= double(q.y);
+        }
+        C2 tn;
+        tn.x = Real(hx);
+        tn.y = Real(hy);
+        prev[gi] = tn;
+        double2 p = a.psi[gi];
+        p.x += cr * hx - ci * hy;
+        p.y += cr * hy + ci * hx;
+        a.psi[gi] = p;
+      }
+    }
+    __syncthreads();  // every read of this tile's buffers is done
+  }
+}
+
+// -------------------------------------------------------------- host glue
+
+using Kernel = void (*)(const PassDev*, OrderArgs);
+
+struct Family {
+  int B = 0, R = 0, nt = 0;
+  size_t smem = 0;
+  Kernel k[4] = {nullptr, nullptr, nullptr, nullptr};
+};
+
+template <typename Real, int B, int R>
+Family family() {
+  using T = Tile<Real, B, R>;
+  Family f;
+  f.B = B;
+  f.R = R;
+  f.nt = T::NT;
+  f.smem = T::kSmem;
+  f.k[PASS_FIRST] = k_tile<Real, B, R, PASS_FIRST>;
+  f.k[PASS_MID] = k_tile<Real, B, R, PASS_MID>;
+  f.k[PASS_LAST] = k_tile<Real, B, R, PASS_LAST>;
+  f.k[PASS_ONLY] = k_tile<Real, B, R, PASS_ONLY>;
+  return f;
+}
+
+const Family& family_for(int precision, int kernel) {
+  static const Family f64 = family<double, 12, 4>();
+  static const Family f32 = family<float, 13, 4>();
+  static const Family s64 = family<double, 8, 3>();
+  static const Family s32 = family<float, 8, 3>();
+  const bool mixed = precision == SS_PRECISION_MIXED;
+  if (kernel == SS_KERNEL_TILED_SMALL) return mixed ? s32 : s64;
+  return mixed ? f32 : f64;
+}
+
+// Builds pass p's table for layouts of R register bits.
+void fill_pass(PassDev* pd, int L, int B, int R, uint32_t tile, const std::vector<int>& owner,
+               int pass, const std::vector<uint32_t>& field_owner, const ss_ham* h,
+               double scale) {
+  std::memset(pd, 0, sizeof(PassDev));
+  int local[32];
+  int nb = 0, no = 0;
+  for (int s = 0; s < L; ++s) {
+    if ((tile >> s) & 1u) {
+      local[s] = nb;
+      pd->tile_pos[nb++] = static_cast<uint32_t>(s);
+    } else {
+      local[s] = -1;
+      pd->outer_pos[no++] = static_cast<uint32_t>(s);
+    }
+  }
+  pd->nouter = no;
+  for (size_t i = 0; i < h->pairs.size(); ++i) {
+    if (owner[i] != pass) continue;
+    const PairTerm& p = h->pairs[i];
+    const double quarter = scale * 0.25;
+    const double ff = quarter * (p.jx + p.jy), fb = quarter * (p.jx - p.jy);
+    const int li = local[p.lo], lj = local[p.hi];  // li < lj: positions keep their order
+    pd->cff[li * B + lj] = std::abs(ff) > kNegligible ? ff : 0.0;
+    pd->cfb[li * B + lj] = std::abs(fb) > kNegligible ? fb : 0.0;
+    if (pd->cfb[li * B + lj] != 0.0) pd->has_fb = 1;
+  }
+  for (int s = 0; s < L; ++s) {
+    if (field_owner[s] != static_cast<uint32_t>(pass)) continue;
+    const double cx = scale * 0.5 * h->fields[3 * s], cy = scale * 0.5 * h->fields[3 * s + 1];
+    if (std::abs(cx) > kNegligible || std::abs(cy) > kNegligible) {
+      pd->ccx[local[s]] = cx;
+      pd->ccy[local[s]] = cy;
+      pd->has_trans = 1;
+    }
+  }
+  // Layout schedule of the tile (Geo<B, R>, written out for run-time B, R).
+  const int G = (B + R - 1) / R;
+  auto base = [&](int g) { return (g + 1) * R <= B ? g * R : B - R; };
+  auto holds = [&](int g, int s) { return s >= base(g) && s < base(g) + R; };
+  auto first_layout = [&](int s) {
+    for (int g = 0; g < G; ++g) {
+      if (holds(g, s)) return g;
+    }
+    return -1;
+  };
+  auto pair_layout = [&](int i, int j) {
+    for (int g = 0; g < G; ++g) {
+      if (holds(g, i) && holds(g, j)) return g;
+    }
+    return first_layout(i);
+  };
+  auto cross_mine = [&](int g, int p) {
+    return first_layout(base(g) + p) == g && !(g < G - 1 && base(g) + p >= B - R);
+  };
+  for (int g = 0; g < G; ++g) {
+    const int b = base(g);
+    for (int p = 0; p < R; ++p) {
+      for (int q = p + 1; q < R; ++q) {
+        const int i = b + p, j = b + q;
+        if (pair_layout(i, j) == g && (pd->cff[i * B + j] != 0.0 || pd->cfb[i * B + j] != 0.0)) {
+          pd->rmask[g] |= 1u << (p * R + q);
+        }
+      }
+      if (!cross_mine(g, p)) continue;
+      for (int j = b + R; j < B; ++j) {
+        const int i = b + p;
+        if (pd->cff[i * B + j] != 0.0 || pd->cfb[i * B + j] != 0.0) pd->jmask[g] |= 1u << j;
+      }
+    }
+  }
+}
+
+}  // namespace tiled
+
+// Per-Hamiltonian device tables of the tiled kernel.
+struct TiledTables {
+  int precision = -1, kernel = -1, nspins = 0;
+  double scale = 0.0;
+  bool valid = false;
+  std::vector<uint32_t> plan;
+  tiled::PassDev* dev = nullptr;
+};
+
+std::vector<uint32_t> tile_plan(int nspins, int tile_bits) {
+  static std::mutex mu;
+  static std::map<std::pair<int, int>, std::vector<uint32_t>> cache;
+  require(nspins >= 1 && nspins <= kMaxSpins, SS_ERR_OUT_OF_RANGE,
+          "number of spins must be in [1, kMaxSpins]");
+  require(tile_bits >= 2 && tile_bits <= tiled::kMaxTile, SS_ERR_INVALID_ARGUMENT,
+          "tile width out of range");
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = cache.find({nspins, tile_bits});
+  if (it != cache.end()) return it->second;
+  std::vector<uint32_t> p = tiled::make_plan(nspins, tile_bits);
+  require(tiled::covers(nspins, p), SS_ERR_RUNTIME, "tile plan does not cover every pair");
+  for (uint32_t m : p) {
+    require(__builtin_popcount(m) == std::min(nspins, tile_bits), SS_ERR_RUNTIME,
+            "tile plan has a tile of the wrong width");
+  }
+  cache.emplace(std::make_pair(nspins, tile_bits), p);
+  return p;
+}
+
+int tile_bits_for(int precision, int kernel) {
+  return tiled::family_for(precision, kernel).B;
+}
+
+void tiled_release(ss_ham* h) {
+  if (h->tiled == nullptr) return;
+  cudaFree(h->tiled->dev);
+  delete h->tiled;
+  h->tiled = nullptr;
+}
+
+const void* tiled_prepare(ss_ham* h, double scale, int precision, int kernel) {
+  const tiled::Family& f = tiled::family_for(precision, kernel);
+  const int L = h->nspins;
+  require(L >= f.B, SS_ERR_INVALID_ARGUMENT, "the tiled kernel needs at least one full tile");
+  {
+    // Opt in to the tile's shared memory once per kernel, outside any capture.
+    static std::mutex mu;
+    static std::map<tiled::Kernel, bool> configured;
+    std::lock_guard<std::mutex> lock(mu);
+    for (tiled::Kernel k : f.k) {
+      if (!configured[k]) {
+        SS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(f.smem)));
+        configured[k] = true;
+      }
+    }
+  }
+  if (h->tiled == nullptr) h->tiled = new TiledTables;
+  TiledTables* tt = h->tiled;
+  if (tt->precision != precision || tt->kernel != kernel || tt->nspins != L) {
+    std::vector<uint32_t> plan = tile_plan(L, f.B);
+    if (tt->dev == nullptr || plan.size() > tt->plan.size()) {
+      sync(h->engine);
+      cudaFree(tt->dev);
+      tt->dev = nullptr;
+      SS_CUDA(cudaMalloc(&tt->dev, sizeof(tiled::PassDev) * plan.size()));
+    }
+    tt->plan = std::move(plan);
+    tt->precision = precision;
+    tt->kernel = kernel;
+    tt->nspins = L;
+    tt->valid = false;
+  }
+  if (!tt->valid || tt->scale != scale || !h->tiled_terms_valid) {
+    const int P = static_cast<int>(tt->plan.size());
+    // Each coupling to the pass holding both spins that has the fewest so
+    // far; each field to the first pass holding its spin.
+    std::vector<int> owner(h->pairs.size(), -1), load(P, 0);
+    for (size_t i = 0; i < h->pairs.size(); ++i) {
+      const uint32_t m = (1u << h->pairs[i].lo) | (1u << h->pairs[i].hi);
+      for (int p = 0; p < P; ++p) {
+        if ((tt->plan[p] & m) == m && (owner[i] < 0 || load[p] < load[owner[i]])) owner[i] = p;
+      }
+      ++load[owner[i]];
+    }
+    std::vector<uint32_t> field_owner(L, 0);
+    for (int s = 0; s < L; ++s) {
+      for (int p = 0; p < P; ++p) {
+        if ((tt->plan[p] >> s) & 1u) {
+          field_owner[s] = static_cast<uint32_t>(p);
+          break;
+        }
+      }
+    }
+    std::vector<tiled::PassDev> host(P);
+    for (int p = 0; p < P; ++p) {
+      tiled::fill_pass(&host[p], L, f.B, f.R, tt->plan[p], owner, p, field_owner, h, scale);
+    }
+    // Pageable source: staged before the call returns.
+    SS_CUDA(cudaMemcpyAsync(tt->dev, host.data(), sizeof(tiled::PassDev) * P,
+                            cudaMemcpyHostToDevice, h->engine->stream));
+    tt->scale = scale;
+    tt->valid = true;
+    h->tiled_terms_valid = true;
+  }
+  return tt->dev;
+}
+
+void tiled_order(ss_ham* h, int precision, int kernel, const void* cur, void* prev, void* part,
+                 double2* psi, int first, double cr, double ci) {
+  const tiled::Family& f = tiled::family_for(precision, kernel);
+  TiledTables* tt = h->tiled;
+  ss_engine* e = h->engine;
+  const int P = static_cast<int>(tt->plan.size());
+  tiled::OrderArgs a;
+  a.cur = cur;
+  a.prev = prev;
+  a.part = part;
+  a.psi = psi;
+  a.diag = h->diag;
+  a.dscale = tt->scale;
+  a.cr = cr;
+  a.ci = ci;
+  a.first = first;
+  a.ntiles = 1u << (h->nspins - f.B);
+  const unsigned int grid = std::min<unsigned int>(a.ntiles, static_cast<unsigned int>(e->sm_count));
+  for (int p = 0; p < P; ++p) {
+    const int kind = P == 1 ? tiled::PASS_ONLY
+                     : p == 0 ? tiled::PASS_FIRST
+                     : p == P - 1 ? tiled::PASS_LAST
+                                  : tiled::PASS_MID;
+    launch(e, f.k[kind], grid, f.nt, f.smem, static_cast<const tiled::PassDev*>(tt->dev + p), a);
+  }
+}
+
+}  // namespace ss
+
+using namespace ss;
+
+extern "C" {
+
+int ss_tile_plan(int nspins, int tile_bits, int32_t* npass, uint32_t* masks, int32_t cap) {
+  return guarded([&] {
+    require(npass != nullptr, SS_ERR_INVALID_ARGUMENT, "null output");
+    const std::vector<uint32_t> p = tile_plan(nspins, tile_bits);
+    *npass = static_cast<int32_t>(p.size());
+    if (masks != nullptr) {
+      require(cap >= static_cast<int32_t>(p.size()), SS_ERR_INVALID_ARGUMENT,
+              "mask buffer too small");
+      std::copy(p.begin(), p.end(), masks);
+    }
+  });
+}
+
+}  // extern "C"

@@ -169,37 +169,64 @@ def long_run(args) -> dict:
 
 
 def plain(args) -> dict:
-    """The plain FP64 path's kernels on single large vectors: the fused
-    Chebyshev-order kernel at each L (effective bandwidth at the algorithmic
-    80 B per amplitude-order, and anti-aligned pair terms applied per
-    second), and the streaming StateVector kernels at L = 26 (1 GiB vectors),
-    which have no partner gathers."""
-    from . import Hamiltonian, Propagator, StateVector
+    """The plain path's kernels on single large vectors.  For each L and each
+    (precision, kernel family): milliseconds per Chebyshev order, the
+    effective bandwidth at the algorithmic bytes per amplitude-order (80 B
+    FP64, 56 B mixed: T_{n-1}, T_{n-2}, T_n, psi read and write; +8 B for the
+    streamed diagonal is not counted), the DRAM bytes the tiled kernel's
+    passes move by construction (48 P + 40 / 24 P + 40 B), anti-aligned pair
+    terms applied per second, and the mixed result's deviation from FP64 after
+    the timed steps.  Then the streaming StateVector kernels at L = 26 (1 GiB
+    vectors), which have no partner gathers."""
+    from . import Hamiltonian, Propagator, StateVector, tile_plan
     eng = Engine(0)
     stream, e0, e1 = _events(eng)
     rep = {"order_kernel": {}, "streaming": {}}
+    combos = [("fp64", abi.FP64, "gather", abi.KERNEL_GATHER),
+              ("fp64", abi.FP64, "tiled", abi.KERNEL_TILED),
+              ("mixed", abi.MIXED, "gather", abi.KERNEL_GATHER),
+              ("mixed", abi.MIXED, "tiled", abi.KERNEL_TILED)]
     for L in args.sizes:
         spec = workloads.long_propagation(nspins=L, steps=1, every=1, epsilon=1e-7)
         cfg = spec.config()
         s = realization_setup(cfg, 0, L)
         ham = Hamiltonian(eng, L, s["fields"], s["pairs"], s["J"])
-        psi = StateVector(eng, L, s["psi0"])
-        prop = Propagator(L, 1e-7)
-        prop.evolve(ham, abi.REAL, psi, 0.1, 1)          # warm-up, builds the tables
-        eng.synchronize()
-        e0.record(stream)
-        prop.evolve(ham, abi.REAL, psi, 0.1, args.steps)
-        e1.record(stream)
-        e1.synchronize()
-        sec = e0.elapsed_time(e1) / 1e3
-        orders = prop.last_order * args.steps
         amps = float(1 << L)
         npairs = len(s["pairs"]) // 2
-        rep["order_kernel"][int(L)] = {
-            "orders": int(orders), "ms_per_order": 1e3 * sec / orders,
-            "effective_gbs_at_80B": 80.0 * amps * orders / sec / 1e9,
-            "pair_terms_per_s": 0.5 * npairs * amps * orders / sec, "pairs": npairs}
-        del psi, ham
+        out = {"pairs": npairs}
+        final = {}
+        for pname, prec, kname, kern in combos:
+            if kname in args.skip or (kname == "gather" and L > args.gather_max):
+                continue
+            psi = StateVector(eng, L, s["psi0"])
+            prop = Propagator(L, 1e-7, prec, kern)
+            prop.evolve(ham, abi.REAL, psi, 0.1, 1)          # warm-up, builds the tables
+            eng.synchronize()
+            e0.record(stream)
+            prop.evolve(ham, abi.REAL, psi, 0.1, args.steps)
+            e1.record(stream)
+            e1.synchronize()
+            sec = e0.elapsed_time(e1) / 1e3
+            orders = prop.last_order * args.steps
+            alg = 80.0 if prec == abi.FP64 else 56.0
+            r = {"orders": int(orders), "ms_per_order": 1e3 * sec / orders,
+                 "effective_gbs": alg * amps * orders / sec / 1e9, "algorithmic_bytes": alg,
+                 "pair_terms_per_s": 0.5 * npairs * amps * orders / sec}
+            if kname == "tiled":
+                P = len(tile_plan(L, 12 if prec == abi.FP64 else 13))
+                r["passes"] = P
+                r["pass_bytes"] = (48.0 * P + 40.0) if prec == abi.FP64 else (24.0 * P + 40.0)
+                r["pass_gbs"] = r["pass_bytes"] * amps * orders / sec / 1e9
+            final[(pname, kname)] = psi.download()
+            out[f"{pname}_{kname}"] = r
+            del psi
+        ref = final.get(("fp64", "gather"), final.get(("fp64", "tiled")))
+        for key, v in final.items():
+            if ref is not None and key != ("fp64", "gather"):
+                out[f"{key[0]}_{key[1]}"]["max_dev_vs_fp64"] = float(np.abs(v - ref).max())
+        rep["order_kernel"][int(L)] = out
+        del ham
+        print(json.dumps({int(L): out}), flush=True)
     L = 26
     a = StateVector(eng, L)
     b = StateVector(eng, L)
@@ -291,6 +318,9 @@ def main(argv=None) -> None:
     pl = sub.add_parser("plain")
     pl.add_argument("--sizes", type=int, nargs="+", default=[16, 20, 22, 24])
     pl.add_argument("--steps", type=int, default=2)
+    pl.add_argument("--skip", nargs="*", default=[], help="kernel families to leave out")
+    pl.add_argument("--gather-max", type=int, default=30,
+                    help="largest L timed with the gather kernel")
     pl.add_argument("--out", default="")
     ps = sub.add_parser("per_size")
     ps.add_argument("--sizes", type=int, nargs="+", default=[12, 14, 16])
