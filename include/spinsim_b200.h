@@ -306,10 +306,14 @@ int ss_measure_energy(const ss_ham* ham, const ss_state* psi, double* out);
  * vectors (2*2^nspins doubles each, re/im interleaved, 16-byte aligned, on
  * the current device), allocating nothing.  Its scratch is a fixed ~19 KB
  * array in the library's device memory; nspins outside [1, 30] is rejected
- * with SS_ERR_OUT_OF_RANGE.  `stream` is a cudaStream_t (NULL = the legacy
- * default stream); the call waits for it.  The first call on each device
- * looks the scratch up (make it before any stream capture).  Calls that
- * overlap on one device race on the scratch: serialise them. */
+ * with SS_ERR_OUT_OF_RANGE, and a vector whose allocation ends before its
+ * 2*2^nspins doubles with SS_ERR_INVALID_ARGUMENT.  `stream` is a
+ * cudaStream_t (NULL = the legacy default stream); the call waits for it.
+ * The first successful call on each device looks the scratch up (make it
+ * before any stream capture; a failed look-up is retried by the next call)
+ * and keeps its address for the life of the process, so the device's
+ * primary context must not be reset in between.  Calls that overlap on one
+ * device race on the scratch: serialise them. */
 int ss_measure_corr_noalloc(const double* psi, const double* ref, int nspins,
                             int axis, void* stream, double out[2]);
 

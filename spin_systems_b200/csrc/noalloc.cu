@@ -11,10 +11,14 @@
 // The counter must be zero when a launch starts: static device memory is
 // zero at module load and the last block of every launch puts it back to
 // zero.  Calls that overlap on one device (two streams, two host threads)
-// share this scratch and race; the caller serialises them.
+// share this scratch and race; the caller serialises them.  Each vector is
+// checked to lie in device memory of the current device, 16-byte aligned,
+// with its 2 * 2^nspins doubles inside one allocation.
+#include <cuda.h>
+
 #include <mutex>
 
-#include "common.cuh"
+#include "observables.cuh"
 
 namespace ss {
 namespace {
@@ -31,62 +35,66 @@ struct NoAllocScratch {
 
 static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
 
-// Device address of g_noalloc_scratch per device, looked up once per device
-// (the first call on a device does this, with that device current).
+// Device address of g_noalloc_scratch per device, looked up with that device
+// current by the first call on it that succeeds (a failed lookup, e.g. one
+// made during a stream capture, is not remembered: the next call retries).
+// The address stays valid while the device's primary context lives; it is
+// kept for the life of the process.
 NoAllocScratch* g_scratch_addr[kNoAllocMaxDevices] = {};
-std::once_flag g_scratch_once[kNoAllocMaxDevices];
-cudaError_t g_scratch_rc[kNoAllocMaxDevices] = {};
+std::mutex g_scratch_mu[kNoAllocMaxDevices];
 
 NoAllocScratch* scratch_for_current_device() {
   int dev = -1;
   SS_CUDA(cudaGetDevice(&dev));
   require(dev >= 0 && dev < kNoAllocMaxDevices, SS_ERR_RUNTIME,
           "device ordinal beyond the no-allocation scratch table");
-  std::call_once(g_scratch_once[dev], [dev] {
+  std::lock_guard<std::mutex> lock(g_scratch_mu[dev]);
+  if (g_scratch_addr[dev] == nullptr) {
     void* p = nullptr;
-    g_scratch_rc[dev] = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (g_scratch_rc[dev] == cudaSuccess) g_scratch_addr[dev] = static_cast<NoAllocScratch*>(p);
-  });
-  if (g_scratch_rc[dev] != cudaSuccess) {
-    fail(SS_ERR_CUDA, std::string("cudaGetSymbolAddress of the correlator scratch failed: ") +
-                          cudaGetErrorString(g_scratch_rc[dev]));
+    const cudaError_t rc = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (rc != cudaSuccess) {
+      cudaGetLastError();
+      fail(SS_ERR_CUDA, std::string("cudaGetSymbolAddress of the correlator scratch failed: ") +
+                            cudaGetErrorString(rc));
+    }
+    g_scratch_addr[dev] = static_cast<NoAllocScratch*>(p);
   }
   return g_scratch_addr[dev];
 }
 
-// Same arithmetic, in the same order, as the engine's correlator kernel.
+// Same per-thread sums, in the same order, as the engine's correlator kernel
+// (observables.cuh), reduced into the static scratch.
 __global__ void k_corr_noalloc(const double2* __restrict__ psi, const double2* __restrict__ ref,
                                int nspins, int axis, size_t n, NoAllocScratch* scratch) {
-  double re = 0.0, im = 0.0;
-  for (size_t k = blockIdx.x * size_t{blockDim.x} + threadIdx.x; k < n;
-       k += size_t{gridDim.x} * blockDim.x) {
-    double sr = 0.0, si = 0.0;
-    for (int s = 0; s < nspins; ++s) {
-      const size_t mask = size_t{1} << s;
-      double2 t;
-      if (axis == SS_AXIS_Z) {
-        const double2 a = psi[k];
-        t = (k & mask) ? a : make_double2(-a.x, -a.y);
-      } else {
-        const double2 p = psi[k ^ mask];
-        if (axis == SS_AXIS_X) {
-          t = p;
-        } else {
-          t = (k & mask) ? make_double2(p.y, -p.x) : make_double2(-p.y, p.x);
-        }
-      }
-      sr += t.x;
-      si += t.y;
-    }
-    const double2 r = ref[k];
-    re += r.x * sr + r.y * si;
-    im += r.x * si - r.y * sr;
-  }
-  grid_reduce2<kReduceThreads>(make_double2(re, im), scratch->partials, &scratch->counter,
-                               &scratch->result);
+  grid_reduce2<kReduceThreads>(corr_thread_sum(psi, ref, nspins, axis, n), scratch->partials,
+                               &scratch->counter, &scratch->result);
 }
 
-void check_vector(const double* p, int dev, const char* what) {
+// The driver's cuMemGetAddressRange, fetched through the runtime (the
+// library links no driver library): the allocation holding a pointer.
+using AddressRangeFn = CUresult (*)(CUdeviceptr*, size_t*, CUdeviceptr);
+
+AddressRangeFn address_range_fn() {
+  static std::once_flag once;
+  static AddressRangeFn fn = nullptr;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess) {
+      fn = reinterpret_cast<AddressRangeFn>(p);
+    } else {
+      cudaGetLastError();
+    }
+  });
+  require(fn != nullptr, SS_ERR_RUNTIME, "cuMemGetAddressRange is not available");
+  return fn;
+}
+
+// A state vector the kernel may read: device (or managed) memory of the
+// current device, 16-byte aligned, and `bytes` long inside one allocation.
+void check_vector(const double* p, int dev, size_t bytes, const char* what) {
   require(p != nullptr, SS_ERR_INVALID_ARGUMENT, "null state pointer");
   require(reinterpret_cast<uintptr_t>(p) % 16 == 0, SS_ERR_INVALID_ARGUMENT,
           "state pointer is not 16-byte aligned");
@@ -97,6 +105,16 @@ void check_vector(const double* p, int dev, const char* what) {
   }
   require(a.device == dev, SS_ERR_INVALID_ARGUMENT,
           "state lives on another device than the current one");
+  CUdeviceptr base = 0;
+  size_t size = 0;
+  const CUdeviceptr at = reinterpret_cast<CUdeviceptr>(p);
+  if (address_range_fn()(&base, &size, at) != CUDA_SUCCESS) {
+    fail(SS_ERR_INVALID_ARGUMENT, std::string(what) + " is not inside a device allocation");
+  }
+  if (at - base > size || size - (at - base) < bytes) {
+    fail(SS_ERR_INVALID_ARGUMENT,
+         std::string(what) + " is shorter than 2 * 2^nspins doubles (its allocation ends first)");
+  }
 }
 
 }  // namespace
@@ -118,8 +136,8 @@ extern "C" int ss_measure_corr_noalloc(const double* psi, const double* ref, int
     NoAllocScratch* scratch = scratch_for_current_device();
     int dev = -1;
     SS_CUDA(cudaGetDevice(&dev));
-    check_vector(psi, dev, "psi");
-    check_vector(ref, dev, "ref");
+    check_vector(psi, dev, n * sizeof(double2), "psi");
+    check_vector(ref, dev, n * sizeof(double2), "ref");
     auto s = static_cast<cudaStream_t>(stream);
     k_corr_noalloc<<<blocks, kReduceThreads, 0, s>>>(reinterpret_cast<const double2*>(psi),
                                                       reinterpret_cast<const double2*>(ref),

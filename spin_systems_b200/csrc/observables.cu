@@ -4,39 +4,17 @@
 //   mag:<s:a> <psi| sigma_a(s) |psi>             (re)
 //   energy    <psi| H |psi>                      (re)
 #include "hamiltonian.cuh"
+#include "observables.cuh"
 
 namespace ss {
 namespace {
-
-__device__ __forceinline__ double2 sigma_at(const double2* __restrict__ in, size_t k, size_t mask,
-                                            int axis) {
-  if (axis == SS_AXIS_Z) {
-    const double2 a = in[k];
-    return (k & mask) ? a : make_double2(-a.x, -a.y);
-  }
-  const double2 p = in[k ^ mask];
-  if (axis == SS_AXIS_X) return p;
-  return (k & mask) ? make_double2(p.y, -p.x) : make_double2(-p.y, p.x);
-}
 
 // <ref|A psi> with A = sum_s sigma_axis(s): conj(ref_k) (A psi)_k summed.
 __global__ void k_corr(const double2* __restrict__ psi, const double2* __restrict__ ref,
                        int nspins, int axis, size_t n, double2* partials, unsigned int* counter,
                        double2* result) {
-  double re = 0.0, im = 0.0;
-  for (size_t k = blockIdx.x * size_t{blockDim.x} + threadIdx.x; k < n;
-       k += size_t{gridDim.x} * blockDim.x) {
-    double sr = 0.0, si = 0.0;
-    for (int s = 0; s < nspins; ++s) {
-      const double2 t = sigma_at(psi, k, size_t{1} << s, axis);
-      sr += t.x;
-      si += t.y;
-    }
-    const double2 r = ref[k];
-    re += r.x * sr + r.y * si;
-    im += r.x * si - r.y * sr;
-  }
-  grid_reduce2<kReduceThreads>(make_double2(re, im), partials, counter, result);
+  grid_reduce2<kReduceThreads>(corr_thread_sum(psi, ref, nspins, axis, n), partials, counter,
+                               result);
 }
 
 __global__ void k_mag(const double2* __restrict__ psi, size_t mask, int axis, size_t n,

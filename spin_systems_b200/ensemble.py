@@ -90,9 +90,10 @@ Runner = Callable[[int, int], Tuple[np.ndarray, np.ndarray]]
 
 def run_sharded(runner: Runner, total: int, group=None) -> Optional[Tuple[np.ndarray, Accumulator]]:
     """Runs this rank's shard through `runner(first, count) -> (times, rows)`
-    and folds every rank's rows on rank 0 in index order.
+    and folds every rank's rows on the group's rank 0 in index order.
 
-    Returns (times, accumulator) on rank 0 and None elsewhere.  With no
+    Returns (times, accumulator) on the group's rank 0 and None elsewhere
+    (`group` defaults to the whole world; only its members may call).  With no
     initialised process group it runs everything locally.  Every rank takes
     the same collective steps (one gather), also when its shard is empty."""
     import torch.distributed as dist
@@ -100,10 +101,14 @@ def run_sharded(runner: Runner, total: int, group=None) -> Optional[Tuple[np.nda
         times, rows = runner(0, total)
         return np.asarray(times), fold_rows(rows)
     world, rank = dist.get_world_size(group), dist.get_rank(group)
+    if rank < 0:
+        raise ValueError("this process is not a member of the group")
     first, count = shard(total, world, rank)
     times, rows = runner(first, count) if count else (None, None)
     gathered = [None] * world if rank == 0 else None
-    dist.gather_object((first, times, rows), gathered, dst=0, group=group)
+    # gather_object names its destination by global rank: the group's rank 0.
+    dst = 0 if group is None else dist.get_global_rank(group, 0)
+    dist.gather_object((first, times, rows), gathered, dst=dst, group=group)
     if rank != 0:
         return None
     parts = sorted((p for p in gathered if p[2] is not None), key=lambda p: p[0])

@@ -125,3 +125,49 @@ def test_gloo_ranks_fold_like_one_process(cpmg_rows, tmp_path, world, total):
     assert np.array_equal(got["mean"], want.mean)
     assert np.array_equal(got["sd"], want.standard_deviation())
     assert np.array_equal(got["se"], want.standard_error())
+
+
+def _subgroup_main(rank, world, port, data, total, out):
+    # Ranks 1 and 2 form a group without global rank 0; the group's rank 0
+    # (global rank 1) receives the fold.
+    import torch.distributed as dist
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
+                            world_size=world, timeout=timedelta(seconds=60))
+    try:
+        sub = dist.new_group([1, 2])
+        if rank == 0:
+            return
+        d = np.load(data)
+        times, rows = d["times"], d["rows"]
+        res = run_sharded(lambda first, count: (times, rows[first:first + count]), total,
+                          group=sub)
+        if rank == 1:
+            t, acc = res
+            np.savez(out, times=t, mean=acc.mean, count=acc.count)
+        else:
+            assert res is None
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gloo_subgroup_without_global_rank_zero(cpmg_rows, tmp_path):
+    times, rows = cpmg_rows
+    data = tmp_path / "rows.npz"
+    np.savez(data, times=times, rows=rows)
+    out = tmp_path / "out.npz"
+    ctx = mp.get_context("spawn")
+    port = _free_port()
+    procs = [ctx.Process(target=_subgroup_main, args=(r, 3, port, str(data), len(rows), str(out)))
+             for r in range(3)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+    codes = [p.exitcode for p in procs]
+    for p in procs:
+        if p.is_alive():
+            p.kill()
+    assert codes == [0, 0, 0], codes
+    got = np.load(out)
+    assert int(got["count"]) == len(rows)
+    assert np.array_equal(got["mean"], fold_rows(rows).mean)

@@ -46,13 +46,17 @@ def test_caller_stream_and_no_device_allocation(engine):
     side = torch.cuda.Stream()
     side.wait_stream(torch.cuda.current_stream())
     ss.measure_corr_noalloc(dpsi.data_ptr(), dref.data_ptr(), nspins, 0, side.cuda_stream)
+    side.synchronize()
     free0, _ = torch.cuda.mem_get_info()
+    alloc0, reserved0 = torch.cuda.memory_allocated(), torch.cuda.memory_reserved()
     for _ in range(20):
         got = ss.measure_corr_noalloc(dpsi.data_ptr(), dref.data_ptr(), nspins, 0,
                                       side.cuda_stream)
         assert got == want
     free1, _ = torch.cuda.mem_get_info()
     assert free1 == free0
+    assert torch.cuda.memory_allocated() == alloc0
+    assert torch.cuda.memory_reserved() == reserved0
 
 
 @pytest.mark.gpu
@@ -66,3 +70,19 @@ def test_rejects_host_and_misaligned_pointers(engine):
         ss.measure_corr_noalloc(dev.data_ptr() + 8, dev.data_ptr(), 4, 2)
     with pytest.raises(ss.InvalidArgumentError, match="null state"):
         ss.measure_corr_noalloc(0, dev.data_ptr(), 4, 2)
+
+
+@pytest.mark.gpu
+def test_rejects_a_vector_shorter_than_its_spin_count(engine):
+    # A 4 MiB tensor has a device allocation of its own; a pointer 8 KiB
+    # before its end cannot hold the 16 KiB of a 10-spin vector.
+    import torch
+    buf = torch.zeros(1 << 19, dtype=torch.float64, device="cuda:0")
+    torch.cuda.synchronize()
+    tail = buf.data_ptr() + buf.numel() * 8 - 8192
+    ok = buf.data_ptr() + buf.numel() * 8 - 16384
+    with pytest.raises(ss.InvalidArgumentError, match="shorter than"):
+        ss.measure_corr_noalloc(tail, ok, 10, 0)
+    with pytest.raises(ss.InvalidArgumentError, match="shorter than"):
+        ss.measure_corr_noalloc(ok, tail, 10, 0)
+    assert ss.measure_corr_noalloc(ok, ok, 10, 2) == (0.0, 0.0)
