@@ -43,7 +43,10 @@ SMEM_BYTES_PER_AMP_ORDER = 168.0   # shared-memory traffic of the L=12, R=4 FP32
 # DRAM bytes per amplitude-order of k_batch<12,4,float>: ncu capture of
 # profile_case (296 realisations, 2 XY-8 blocks): 48.2 MB for 6.149e9.
 DRAM_BYTES_PER_AMP_ORDER_MEASURED = 48.215296e6 / 6.149e9
-FLOPS_PER_AMP_ORDER = L * (L - 1) * 2 + 20
+# FP32 flops per amplitude-order: two FMAs for each of the ~L(L-1)/4
+# anti-aligned coupling terms, plus the fields and the recurrence.
+FLOPS_PER_AMP_ORDER = L * (L - 1) + 20
+CPU_SAMPLE_SEED = 0x5EED_C0DE
 
 
 def workload():
@@ -162,27 +165,46 @@ def cpu_threads():
         return os.cpu_count() or 1
 
 
-def reference_sample(spec, steps, warmup, per_step=None):
-    """The reference's own CPU implementation (oracle/_ref when built here,
-    else the C restatement) on the host cores, a bounded sample per step."""
+def cpu_model() -> str:
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def seeded_subset(count, total, seed):
+    """`count` realisation indices from [0, total), drawn without
+    replacement (then again, if more are asked for than exist) from a seeded
+    stream: a sample spread over the whole batch, the same on every run."""
+    rng = np.random.default_rng(seed)
+    out = []
+    while len(out) < count:
+        out.extend(rng.permutation(total)[: count - len(out)].tolist())
+    return np.asarray(out, dtype=np.uint64)
+
+
+def cpu_impl():
     from oracle.oracle import Port, Ref
-    threads = cpu_threads()
-    if Ref.available():
-        lib, kind = Ref(), "reference"
-    else:
-        lib, kind = Port(), "port"
-    cfg = spec.config()
-    n = per_step or threads
-    for _ in range(warmup):
-        lib.run_range(cfg, 0, min(n, threads), threads)
-    total = 0.0
-    for s in range(steps):
-        _, _, secs = lib.run_range(cfg, (s * n) % REALIZATIONS, n, threads)
-        total += secs
-    return {"value": steps * n / total, "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": f"{n} realisations of the L=12 XY-8 workload per step on {threads} threads "
-                      f"(LocalRunner-equivalent thread pool over runRealization)",
-            "seconds": total}
+    return (Ref(), "reference") if Ref.available() else (Port(), "port")
+
+
+def reference_sample(spec, count, threads, seed):
+    """The reference's own CPU implementation (oracle/_ref when built here,
+    else the C restatement) over a seeded subset of the batch's realisations
+    in one pool of `threads` host threads that take the next realisation as
+    they finish (the reference's LocalRunner schedule), so every thread is
+    busy until the sample runs out."""
+    lib, kind = cpu_impl()
+    idx = seeded_subset(count, REALIZATIONS, seed)
+    _, _, secs = lib.run_indices(spec.config(), idx, threads)
+    return {"value": len(idx) / secs, "unit": UNIT, "cores": threads, "kind": kind,
+            "seconds": secs, "realizations": int(len(idx)),
+            "sample": f"{len(idx)} realisations drawn at random (seeded) from the batch's "
+                      f"{REALIZATIONS}, one runRealization pool on {threads} threads",
+            "model": cpu_model()}
 
 
 def run_reference_arm(args):
@@ -190,13 +212,23 @@ def run_reference_arm(args):
     if int(os.environ.get("RANK", "0")) != 0:
         return
     spec = workload()
-    cb = reference_sample(spec, args.steps, args.warmup)
+    threads = cpu_threads()
+    lib, kind = cpu_impl()
+    per_step = threads
+    for w in range(args.warmup):  # untimed: a quarter step each
+        lib.run_indices(spec.config(), seeded_subset(max(1, threads // 4), REALIZATIONS, w),
+                        threads)
+    # The K steps' samples (K x threads realisations across the batch) run as
+    # one pool, so no thread idles at a step boundary waiting for the
+    # slowest realisation of its step.
+    cb = reference_sample(spec, args.steps * per_step, threads, CPU_SAMPLE_SEED)
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * cb["seconds"] / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": config_block(1),
-            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample",
+                                                "model")},
             "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -254,13 +286,23 @@ def run_ours(args):
     dev_ms = barrier_max(world, dev_ms)
     barrier(world)
 
-    # End to end through the C ABI with host buffers: upload of every input,
-    # the run, download of the rows, all inside the timed region.
+    # End to end through the C ABI from the config, as the reference arm
+    # runs: every step assembles the realisations on the host (random
+    # streams, geometry, disorder, initial states, expansions), uploads them
+    # from host buffers, runs, and downloads the rows.
+    e2e_steps = args.steps
     t0 = time.perf_counter()
-    for _ in range(args.steps):
+    for _ in range(e2e_steps):
+        b = ss.Batch(eng, cfg, first, REALIZATIONS, abi.MIXED)
+        times, mixed = b.run()
+        b._destroy()
+    e2e_s = barrier_max(world, time.perf_counter() - t0)
+    # The same with the assembled tables kept: upload, run, download.
+    res_steps = min(args.steps, 3)
+    t0 = time.perf_counter()
+    for _ in range(res_steps):
         times, mixed = batch.run()
-    e2e_s = time.perf_counter() - t0
-    e2e_s = barrier_max(world, e2e_s)
+    res_s = barrier_max(world, time.perf_counter() - t0)
 
     if rank != 0:
         barrier(world)
@@ -280,13 +322,9 @@ def run_ours(args):
     err = np.abs(mixed[:check, :, 0] - fp64[:, :, 0]).max(axis=1) / np.array(corr0)
     del b64
 
-    # Plain FP64 path: one realisation at a time through runRealization.
-    plain_n = 3
-    ss.run_realization(eng, cfg, first, batch.points, batch.width)
-    t0 = time.perf_counter()
-    for i in range(plain_n):
-        ss.run_realization(eng, cfg, first + i, batch.points, batch.width)
-    plain_rate = plain_n / (time.perf_counter() - t0)
+    # Plain FP64 path: one realisation at a time through runRealization, on a
+    # seeded sample spread over the batch (its realisations differ ~10x in work).
+    plain = plain_sample(eng, cfg, first, batch, amp_each, PLAIN_SAMPLE, CPU_SAMPLE_SEED + 1)
 
     value = world * REALIZATIONS * args.steps / (dev_ms / 1e3)
     ms_step = dev_ms / args.steps
@@ -297,43 +335,65 @@ def run_ours(args):
     achieved = alg_bytes / (ms_step / 1e3) / 1e9
     hbm, src = peaks()
     clk = clocks.summary()
-    smem_peak = 128.0 * eng_sms() * (clk["sm_mhz"] or 1965.0) * 1e6 / 1e9
+    mhz = clk["sm_mhz"] or 1965.0
+    smem_peak = 128.0 * eng_sms() * mhz * 1e6 / 1e9
     smem_ach = SMEM_BYTES_PER_AMP_ORDER * amp_mixed / (ms_step / 1e3) / 1e9
-    cb = reference_sample(spec, 1, 0, per_step=max(2, cpu_threads()))
+    fma_peak = 2.0 * 128.0 * eng_sms() * mhz * 1e6 / 1e12
+    fma_ach = FLOPS_PER_AMP_ORDER * amp_mixed / (ms_step / 1e3) / 1e12
+    threads = cpu_threads()
+    cb = reference_sample(spec, 3 * threads, threads, CPU_SAMPLE_SEED + 2)
+    cb1 = reference_sample(spec, 2, 1, CPU_SAMPLE_SEED + 3)
+    sizes = per_size_ratios(eng, args) if args.per_size else {}
+    kern = plain_order_kernels(eng, hbm) if args.plain_kernels else {}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": config_block(world),
-        "e2e": {"value": world * REALIZATIONS * args.steps / e2e_s, "unit": UNIT,
-                "h2d_bytes_per_step": stats["h2d_bytes"], "d2h_bytes_per_step": stats["d2h_bytes"]},
+        "e2e": {"value": world * REALIZATIONS * e2e_steps / e2e_s, "unit": UNIT,
+                "h2d_bytes_per_step": stats["h2d_bytes"], "d2h_bytes_per_step": stats["d2h_bytes"],
+                "includes": "host assembly of every realisation (ss_batch_create), upload from "
+                            "host buffers, run, download of the rows"},
+        "e2e_tables_resident": {"value": world * REALIZATIONS * res_steps / res_s, "unit": UNIT,
+                                "steps": res_steps,
+                                "includes": "upload from host buffers, run, download (tables "
+                                            "assembled once before timing)"},
         "gpu_launches": int(launches),
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm,
+        "roofline": {"bound": "smem", "achieved": smem_ach, "peak": smem_peak, "unit": "GB/s",
+                     "frac": smem_ach / smem_peak,
                      "traffic": DRAM_BYTES_PER_AMP_ORDER_MEASURED * amp_mixed,
                      "traffic_note": "DRAM bytes of the mixed kernel per launch, scaled from "
                                      "an ncu capture of a smaller case by amplitude-orders",
-                     "peak_source": src,
+                     "peak_source": "architectural: 128 B/clk/SM x SMs x the median SM clock "
+                                    "sampled under load (no measured shared-memory peak)",
+                     "bytes_per_amp_order": SMEM_BYTES_PER_AMP_ORDER,
                      "kernel": kernel_desc(tuned),
-                     "algorithmic_bytes_per_launch": alg_bytes,
-                     "note": "effective bandwidth of a shared-memory-resident kernel pair; the "
-                             "binding limit is shared-memory bandwidth and issue (see smem)"},
-        "smem": {"achieved_gbs": smem_ach, "peak_gbs": smem_peak, "frac": smem_ach / smem_peak,
-                 "bytes_per_amp_order": SMEM_BYTES_PER_AMP_ORDER,
-                 "note": "FP32 kernel's share only"},
+                     "binding": "on-chip: the recursion lives in shared memory; shared-memory "
+                                "bandwidth and instruction issue bind, not HBM",
+                     "hbm_effective": {"achieved": achieved, "peak": hbm, "unit": "GB/s",
+                                       "frac": achieved / hbm, "peak_source": src,
+                                       "algorithmic_bytes_per_launch": alg_bytes,
+                                       "note": "algorithmic bytes / time of an on-chip kernel: "
+                                               "an effective bandwidth, not an HBM fraction"},
+                     "fp32_fma": {"achieved_tflops": fma_ach, "peak_tflops": fma_peak,
+                                  "frac": fma_ach / fma_peak,
+                                  "peak_source": "architectural: 128 FP32 FMA/clk/SM x 2 flops "
+                                                 "x SMs x the median SM clock under load"}},
+        "plain_order_kernel_hbm": kern,
         "routing": {"fp64_realizations": int(routed.sum()), "realizations": int(len(prec)),
                     "fp64_amplitude_order_share": amp_fp64 / amp_orders,
                     "rule": "more than 40000 Chebyshev orders per state vector -> FP64 kernel"},
-        "fp32_tflops": FLOPS_PER_AMP_ORDER * amp_mixed / (ms_step / 1e3) / 1e12,
         "clocks": clk,
         "echo_error": {"max": float(err.max()), "mean": float(err.mean()), "curves": check,
                        "above_1e-6": int((err > 1e-6).sum()),
                        "max_mixed_only": float(err[~routed].max()) if (~routed).any() else 0.0,
                        "reference": "batched FP64 on the same realisations"},
-        "plain_fp64": {"value": plain_rate, "unit": UNIT, "curves": plain_n,
-                       "speedup_of_batched_mixed": value / world / plain_rate},
+        "plain_fp64": dict(plain, speedup_of_batched_mixed=value / world / plain["value"]),
+        "per_size_cpmg32": sizes,
         "work": {"amplitude_orders_per_step": amp_orders, "orders_per_step": stats["orders"]},
-        "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "cpu_baseline": dict({k: cb[k] for k in ("value", "unit", "cores", "kind", "sample",
+                                                 "model")},
+                             one_thread={k: cb1[k] for k in ("value", "unit", "sample")}),
         "schedule": ({"tuned": [{k: r[k] for k in ("L", "precision", "variant", "ns")} for r in tuned],
                       "tuning_seconds": tune_s, "sample": args.tune_sample}
                      if args.tune else {"tuned": [], "note": "default schedules (--no-tune)"}),
@@ -343,6 +403,117 @@ def run_ours(args):
     del batch
     eng.close()
 
+
+PLAIN_SAMPLE = 16
+
+
+def plain_sample(eng, cfg, first, batch, amp_each, n, seed):
+    """The plain FP64 path (ss_run_realization, one realisation at a time)
+    on a seeded sample of the batch: its curves/s, and the rate its seconds
+    per amplitude-order give for the whole batch."""
+    import spin_systems_b200 as ss
+    idx = [int(i) for i in seeded_subset(n, REALIZATIONS, seed)]
+    ss.run_realization(eng, cfg, first + idx[0], batch.points, batch.width)  # warm-up
+    secs = 0.0
+    for i in idx:
+        t0 = time.perf_counter()
+        ss.run_realization(eng, cfg, first + i, batch.points, batch.width)
+        secs += time.perf_counter() - t0
+    amp = np.asarray(amp_each, dtype=np.float64)
+    batch_secs = secs * amp.sum() / amp[idx].sum()
+    return {"value": n / secs, "unit": UNIT, "curves": n,
+            "sample": f"{n} realisations drawn at random (seeded) from the batch",
+            "amplitude_order_scaled": len(amp) / batch_secs}
+
+
+def per_size_ratios(eng, args):
+    """The uneven batch's CPMG-32 program (sigma, tau ~ U[0.1, 1]) at one L
+    at a time: the batched mixed engine (tuned for the size) against the
+    plain FP64 path on a seeded sample of the same realisations."""
+    import torch
+    import spin_systems_b200 as ss
+    from spin_systems_b200 import abi, workloads
+    out = {}
+    stream = torch.cuda.ExternalStream(eng.stream, device=torch.device("cuda", 0))
+    for Lx, n in ((14, 296), (16, 120)):
+        spec = workloads.cpmg_uneven(realizations=n)
+        spec.spin_choices = (Lx,)
+        cfg = spec.config()
+        ss.tune(eng, cfg, 0, 32, abi.MIXED)
+        b = ss.Batch(eng, cfg, 0, n, abi.MIXED)
+        b.upload()
+        b.execute()
+        eng.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        b.execute()
+        e1.record(stream)
+        e1.synchronize()
+        sec = e0.elapsed_time(e1) / 1e3
+        _, mixed = b.download()
+        _, amp = b.work()
+        amp = np.asarray(amp, dtype=np.float64)
+        rng = np.random.default_rng(CPU_SAMPLE_SEED + Lx)
+        idx = [int(i) for i in rng.permutation(n)[:8]]
+        psec, errs = 0.0, []
+        ss.run_realization(eng, cfg, idx[0], b.points, b.width)
+        for i in idx:
+            t0 = time.perf_counter()
+            _, rows = ss.run_realization(eng, cfg, i, b.points, b.width)
+            psec += time.perf_counter() - t0
+            scale = max(abs(rows[0, 0]), 1e-300)
+            errs.append(float(np.abs(mixed[i, :, 0] - rows[:, 0]).max() / scale))
+        plain_rate = n / (psec * amp.sum() / amp[idx].sum())
+        out[int(Lx)] = {"realizations": n, "batched_mixed_curves_per_s": n / sec,
+                        "plain_fp64_curves_per_s": plain_rate, "ratio": n / sec / plain_rate,
+                        "plain_sample": len(idx),
+                        "plain_scaling": "seconds per amplitude-order of the seeded sample x "
+                                         "the batch's amplitude-orders",
+                        "echo_error_max": max(errs),
+                        "schedule": {r["precision"]: r["variant"] for r in ss.schedule()
+                                     if r["L"] == Lx}}
+        b._destroy()
+    return out
+
+
+def plain_order_kernels(eng, hbm):
+    """The plain path's order kernel on single vectors larger than L2 (the
+    long-propagation realisation at L = 22 and 24): device time per order,
+    effective bandwidth at the algorithmic 80 B (FP64) / 56 B (mixed) per
+    amplitude-order as a fraction of measured HBM, and the bytes the tiled
+    kernel's passes move by construction."""
+    import torch
+    import spin_systems_b200 as ss
+    from spin_systems_b200 import abi, workloads
+    stream = torch.cuda.ExternalStream(eng.stream, device=torch.device("cuda", 0))
+    out = {}
+    for Lx, prec, name in ((22, abi.FP64, "fp64"), (24, abi.FP64, "fp64"), (24, abi.MIXED, "mixed")):
+        spec = workloads.long_propagation(nspins=Lx, steps=1, every=1, epsilon=1e-7)
+        s = ss.realization_setup(spec.config(), 0, Lx)
+        ham = ss.Hamiltonian(eng, Lx, s["fields"], s["pairs"], s["J"])
+        psi = ss.StateVector(eng, Lx, s["psi0"])
+        prop = ss.Propagator(Lx, 1e-7, prec, abi.KERNEL_TILED)
+        prop.evolve(ham, abi.REAL, psi, 0.1, 1)
+        eng.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        prop.evolve(ham, abi.REAL, psi, 0.1, 1)
+        e1.record(stream)
+        e1.synchronize()
+        sec = e0.elapsed_time(e1) / 1e3
+        orders = prop.last_order
+        alg = 80.0 if prec == abi.FP64 else 56.0
+        P = len(ss.tile_plan(Lx, 12 if prec == abi.FP64 else 13))
+        pbytes = 48.0 * P + 40.0 if prec == abi.FP64 else 24.0 * P + 40.0
+        amps = float(1 << Lx)
+        eff = alg * amps * orders / sec / 1e9
+        out[f"L{Lx}_{name}"] = {"ms_per_order": 1e3 * sec / orders, "effective_gbs": eff,
+                                "frac_of_hbm": eff / hbm, "algorithmic_bytes": alg,
+                                "passes": P, "pass_bytes": pbytes,
+                                "pass_gbs": pbytes * amps * orders / sec / 1e9,
+                                "pair_terms_per_s": 0.5 * len(s["J"]) / 3 * amps * orders / sec}
+        del psi, ham
+    return out
 
 
 def run_cpmg10(args):
@@ -430,6 +601,10 @@ def main():
                     help="run the autotuner before timing (default)")
     ap.add_argument("--no-tune", dest="tune", action="store_false")
     ap.add_argument("--tune-sample", type=int, default=296)
+    ap.add_argument("--no-per-size", dest="per_size", action="store_false", default=True,
+                    help="skip the per-size L = 14 / 16 CPMG-32 ratios")
+    ap.add_argument("--no-plain-kernels", dest="plain_kernels", action="store_false",
+                    default=True, help="skip the plain order kernel at L = 22 / 24")
     ap.add_argument("--workload", choices=["xy8", "cpmg10"], default="xy8",
                     help="xy8: the headline batch (default); cpmg10: the L=10 demo case")
     args = ap.parse_args()

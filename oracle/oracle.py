@@ -190,6 +190,20 @@ class Port(_Lib):
                                            _d(times), _d(values), C.byref(secs)))
         return times[:p], values[: count * p * w].reshape(count, p, w), secs.value
 
+    def run_indices(self, cfg: SsRunConfig, indices, threads: int):
+        """runRealization for each index of `indices` on a thread pool taking
+        the next index as it finishes; rows in list order, wall seconds."""
+        idx = np.ascontiguousarray(indices, dtype=np.uint64)
+        count = len(idx)
+        p, w = self.shape(cfg)
+        times = np.zeros(max(p, 1))
+        values = np.zeros(max(count * p * w, 1))
+        secs = C.c_double()
+        self._check(self.lib.orc_run_indices(C.byref(cfg), idx.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                                 C.c_int64(count), threads, _d(times), _d(values),
+                                                 C.byref(secs)))
+        return times[:p], values[: count * p * w].reshape(count, p, w), secs.value
+
     def accumulate(self, rows):
         rows = np.ascontiguousarray(rows, dtype=np.float64)
         n, w = rows.shape
@@ -315,6 +329,20 @@ class Ref(_Lib):
         secs = C.c_double()
         self._check(self.lib.refd_run_range(C.byref(cfg), C.c_uint64(first), C.c_int64(count), threads,
                                             _d(times), _d(values), C.byref(secs)))
+        return times[:p], values[: count * p * w].reshape(count, p, w), secs.value
+
+    def run_indices(self, cfg: SsRunConfig, indices, threads: int):
+        """runRealization for each index of `indices` on a thread pool taking
+        the next index as it finishes; rows in list order, wall seconds."""
+        idx = np.ascontiguousarray(indices, dtype=np.uint64)
+        count = len(idx)
+        p, w = self.shape(cfg)
+        times = np.zeros(max(p, 1))
+        values = np.zeros(max(count * p * w, 1))
+        secs = C.c_double()
+        self._check(self.lib.refd_run_indices(C.byref(cfg), idx.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                                 C.c_int64(count), threads, _d(times), _d(values),
+                                                 C.byref(secs)))
         return times[:p], values[: count * p * w].reshape(count, p, w), secs.value
 
     def random_state(self, L: int, seed: int):

@@ -406,11 +406,12 @@ int refd_run_realization(const ss_run_config* c, uint64_t index, double* times,
   });
 }
 
-// runRealization for indices [first, first+count) on `threads` host threads,
-// rows stored in index order.  Wall-clock seconds of the parallel region are
-// returned in *seconds.
-int refd_run_range(const ss_run_config* c, uint64_t first, int64_t count, int threads,
-                   double* times, double* values, double* seconds) {
+// runRealization for the `count` realisation indices `indices` on `threads`
+// host threads taking the next index as they finish (the dynamic schedule of
+// the reference's LocalRunner, EnsembleRunner.cpp:27-88), rows stored in list
+// order.  Wall-clock seconds of the parallel region go to *seconds.
+int refd_run_indices(const ss_run_config* c, const uint64_t* indices, int64_t count, int threads,
+                     double* times, double* values, double* seconds) {
   return guarded([&] {
     const RunConfig cfg = toRunConfig(*c);
     std::vector<VectorRecorder> recs(static_cast<std::size_t>(count));
@@ -427,7 +428,7 @@ int refd_run_range(const ss_run_config* c, uint64_t first, int64_t count, int th
             const int64_t i = next.fetch_add(1);
             if (i >= count) return;
             try {
-              runRealization(cfg, static_cast<std::size_t>(first + static_cast<uint64_t>(i)),
+              runRealization(cfg, static_cast<std::size_t>(indices[i]),
                              recs[static_cast<std::size_t>(i)]);
             } catch (...) {
               std::lock_guard lock(m);
@@ -449,6 +450,14 @@ int refd_run_range(const ss_run_config* c, uint64_t first, int64_t count, int th
       at += r.values().size();
     }
   });
+}
+
+// The same for indices [first, first+count).
+int refd_run_range(const ss_run_config* c, uint64_t first, int64_t count, int threads,
+                   double* times, double* values, double* seconds) {
+  std::vector<uint64_t> idx(static_cast<std::size_t>(count > 0 ? count : 0));
+  for (std::size_t i = 0; i < idx.size(); ++i) idx[i] = first + i;
+  return refd_run_indices(c, idx.data(), count, threads, times, values, seconds);
 }
 
 // runExperiment (io/Experiment.cpp:57-72) with LocalRunner(threads): mean,

@@ -894,6 +894,7 @@ int orc_run_realization(const ss_run_config* c, uint64_t index, double* times, d
 
 typedef struct range_job {
   const ss_run_config* cfg;
+  const uint64_t* indices; /* NULL: first + i */
   uint64_t first;
   int64_t count;
   int64_t points, width;
@@ -913,7 +914,8 @@ static void* range_worker(void* arg) {
     const int stop = j->rc != 0;
     pthread_mutex_unlock(&j->lock);
     if (i >= j->count || stop) break;
-    const int rc = orc_run_realization(j->cfg, j->first + (uint64_t)i, t,
+    const uint64_t index = j->indices ? j->indices[i] : j->first + (uint64_t)i;
+    const int rc = orc_run_realization(j->cfg, index, t,
                                        j->values + i * j->points * j->width);
     if (rc) {
       pthread_mutex_lock(&j->lock);
@@ -927,6 +929,22 @@ static void* range_worker(void* arg) {
   return NULL;
 }
 
+static int run_job(range_job* j, int threads, double* seconds) {
+  orc_shape(j->cfg, &j->points, &j->width);
+  pthread_mutex_init(&j->lock, NULL);
+  if (threads <= 0) threads = 1;
+  pthread_t* pool = malloc(sizeof(pthread_t) * (size_t)threads);
+  struct timespec t0, t1;
+  clock_gettime(CLOCK_MONOTONIC, &t0);
+  for (int i = 0; i < threads; ++i) pthread_create(&pool[i], NULL, range_worker, j);
+  for (int i = 0; i < threads; ++i) pthread_join(pool[i], NULL);
+  clock_gettime(CLOCK_MONOTONIC, &t1);
+  *seconds = (double)(t1.tv_sec - t0.tv_sec) + 1e-9 * (double)(t1.tv_nsec - t0.tv_nsec);
+  free(pool);
+  pthread_mutex_destroy(&j->lock);
+  return j->rc;
+}
+
 int orc_run_range(const ss_run_config* c, uint64_t first, int64_t count, int threads,
                   double* times, double* values, double* seconds) {
   range_job j;
@@ -934,21 +952,21 @@ int orc_run_range(const ss_run_config* c, uint64_t first, int64_t count, int thr
   j.cfg = c;
   j.first = first;
   j.count = count;
-  orc_shape(c, &j.points, &j.width);
   j.times = times;
   j.values = values;
-  pthread_mutex_init(&j.lock, NULL);
-  if (threads <= 0) threads = 1;
-  pthread_t* pool = malloc(sizeof(pthread_t) * (size_t)threads);
-  struct timespec t0, t1;
-  clock_gettime(CLOCK_MONOTONIC, &t0);
-  for (int i = 0; i < threads; ++i) pthread_create(&pool[i], NULL, range_worker, &j);
-  for (int i = 0; i < threads; ++i) pthread_join(pool[i], NULL);
-  clock_gettime(CLOCK_MONOTONIC, &t1);
-  *seconds = (double)(t1.tv_sec - t0.tv_sec) + 1e-9 * (double)(t1.tv_nsec - t0.tv_nsec);
-  free(pool);
-  pthread_mutex_destroy(&j.lock);
-  return j.rc;
+  return run_job(&j, threads, seconds);
+}
+
+int orc_run_indices(const ss_run_config* c, const uint64_t* indices, int64_t count, int threads,
+                    double* times, double* values, double* seconds) {
+  range_job j;
+  memset(&j, 0, sizeof j);
+  j.cfg = c;
+  j.indices = indices;
+  j.count = count;
+  j.times = times;
+  j.values = values;
+  return run_job(&j, threads, seconds);
 }
 
 void orc_accumulate(int64_t n, int64_t width, const double* rows, double* mean, double* sd,

@@ -96,6 +96,9 @@ int orc_run_realization(const ss_run_config* cfg, uint64_t index, double* times,
    rows in index order; wall-clock seconds of the parallel part. */
 int orc_run_range(const ss_run_config* cfg, uint64_t first, int64_t count,
                   int threads, double* times, double* values, double* seconds);
+/* The same over an explicit list of realisation indices (rows in list order). */
+int orc_run_indices(const ss_run_config* cfg, const uint64_t* indices, int64_t count,
+                    int threads, double* times, double* values, double* seconds);
 
 /* Welford / Chan accumulator over rows (Ensemble.cpp:116-166): folds `n`
    rows of `width` in order and writes mean, sd, stderr. */

@@ -26,6 +26,7 @@ def test_reference_arm_prints_the_contract_line():
     assert line["value"] > 0 and line["ms_per_step"] > 0
     cb = line["cpu_baseline"]
     assert cb["value"] == line["value"] and cb["kind"] in ("reference", "port") and cb["cores"] >= 1
+    assert cb["model"] and "seeded" in cb["sample"]
     assert line["e2e"] == {"value": line["value"], "unit": line["unit"],
                            "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     assert "workload" in line["config"]
@@ -34,3 +35,14 @@ def test_reference_arm_prints_the_contract_line():
 def test_reference_arm_other_ranks_exit_without_work():
     out = run_arm({"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"})
     assert out.returncode == 0 and out.stdout.strip() == ""
+
+
+def test_cpu_sample_is_seeded_and_spread_over_the_batch():
+    sys.path.insert(0, str(ROOT))
+    import numpy as np
+    import bench
+    a = bench.seeded_subset(320, 1024, 7)
+    assert np.array_equal(a, bench.seeded_subset(320, 1024, 7))
+    assert len(set(a.tolist())) == 320 and a.max() < 1024 and a.max() > 900 and a.min() < 100
+    b = bench.seeded_subset(1500, 1024, 7)  # more than exist: every index, then again
+    assert len(b) == 1500 and len(set(b[:1024].tolist())) == 1024

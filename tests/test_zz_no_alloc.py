@@ -74,15 +74,21 @@ def test_rejects_host_and_misaligned_pointers(engine):
 
 @pytest.mark.gpu
 def test_rejects_a_vector_shorter_than_its_spin_count(engine):
-    # A 4 MiB tensor has a device allocation of its own; a pointer 8 KiB
-    # before its end cannot hold the 16 KiB of a 10-spin vector.
-    import torch
-    buf = torch.zeros(1 << 19, dtype=torch.float64, device="cuda:0")
-    torch.cuda.synchronize()
-    tail = buf.data_ptr() + buf.numel() * 8 - 8192
-    ok = buf.data_ptr() + buf.numel() * 8 - 16384
-    with pytest.raises(ss.InvalidArgumentError, match="shorter than"):
-        ss.measure_corr_noalloc(tail, ok, 10, 0)
-    with pytest.raises(ss.InvalidArgumentError, match="shorter than"):
-        ss.measure_corr_noalloc(ok, tail, 10, 0)
-    assert ss.measure_corr_noalloc(ok, ok, 10, 2) == (0.0, 0.0)
+    # One exact-size cudaMalloc of 64 KiB (torch's allocator would carve a
+    # tensor out of a larger segment, which the check rightly accepts): a
+    # pointer 8 KiB before its end cannot hold the 16 KiB of a 10-spin vector.
+    from cuda.bindings import runtime as rt
+    err, base = rt.cudaMalloc(1 << 16)
+    assert err == rt.cudaError_t.cudaSuccess
+    try:
+        rc, = rt.cudaMemset(base, 0, 1 << 16)
+        assert rc == rt.cudaError_t.cudaSuccess
+        tail = int(base) + (1 << 16) - 8192
+        ok = int(base) + (1 << 16) - 16384
+        with pytest.raises(ss.InvalidArgumentError, match="shorter than"):
+            ss.measure_corr_noalloc(tail, ok, 10, 0)
+        with pytest.raises(ss.InvalidArgumentError, match="shorter than"):
+            ss.measure_corr_noalloc(ok, tail, 10, 0)
+        assert ss.measure_corr_noalloc(ok, ok, 10, 2) == (0.0, 0.0)
+    finally:
+        rt.cudaFree(base)
