@@ -503,8 +503,8 @@ def plain_order_kernels(eng, hbm):
         sec = e0.elapsed_time(e1) / 1e3
         orders = prop.last_order
         alg = 80.0 if prec == abi.FP64 else 56.0
-        P = len(ss.tile_plan(Lx, 12 if prec == abi.FP64 else 13))
-        pbytes = 48.0 * P + 40.0 if prec == abi.FP64 else 24.0 * P + 40.0
+        P = len(ss.tiled_plan(Lx, prec))
+        pbytes = 48.0 * P + 24.0 if prec == abi.FP64 else 24.0 * P + 24.0
         amps = float(1 << Lx)
         eff = alg * amps * orders / sec / 1e9
         out[f"L{Lx}_{name}"] = {"ms_per_order": 1e3 * sec / orders, "effective_gbs": eff,

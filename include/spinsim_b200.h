@@ -279,11 +279,18 @@ int ss_propagate_ex(const ss_ham* ham, ss_state* psi, int mode, double tau,
                     int64_t nsteps, int autonormalize, double epsilon,
                     int precision, int kernel, int64_t* order_used);
 /* Host only, no counterpart in the reference: the tile patterns of
- * SS_KERNEL_TILED for an nspins-spin vector and tiles of tile_bits spins,
- * one bit mask per pass (every pair of spins shares a pattern; the last pass
- * forms T_n).  *npass receives the count; masks (capacity cap) may be NULL. */
-int ss_tile_plan(int nspins, int tile_bits, int32_t* npass, uint32_t* masks,
-                 int32_t cap);
+ * SS_KERNEL_TILED for an nspins-spin vector and tiles of tile_bits spins
+ * that all hold spins 0 .. line_bits-1 (the tiled kernel uses 12 and 3 in
+ * FP64, 13 and 4 in mixed precision: whole 128-byte runs), one bit mask per
+ * pass (every pair of spins shares a pattern; the last pass forms T_n).
+ * *npass receives the count; masks (capacity cap) may be NULL. */
+int ss_tile_plan(int nspins, int tile_bits, int line_bits, int32_t* npass,
+                 uint32_t* masks, int32_t cap);
+/* No counterpart in the reference: the schedule of SS_KERNEL_TILED per
+ * precision, as register bits per thread (FP64: 3 or 4, mixed: 4 or 5; 0 =
+ * the default, the faster on B200).  Process-wide; results are the same for
+ * every choice up to the order of the sums. */
+int ss_tiled_select(int precision, int register_bits);
 
 /* ------------------------------------------------------------ gates
  * src/core/Gate.cpp:20-33 Rotation2x2::make; :60-85 SpinRotation::apply;

@@ -92,8 +92,8 @@ def load(path: Path = LIB_PATH) -> C.CDLL:
                                  C.c_int64, C.c_int, C.c_int, C.c_int]
     lib.ss_propagate_ex.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_int64,
                                     C.c_int, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_int64)]
-    lib.ss_tile_plan.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_uint32),
-                                 C.c_int32]
+    lib.ss_tile_plan.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int32),
+                                 C.POINTER(C.c_uint32), C.c_int32]
     lib.ss_bessel.argtypes = [C.c_int, C.c_double, C.c_int64, _dp, C.POINTER(C.c_int64)]
     lib.ss_chebyshev_build.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_int64, _dp,
                                        C.c_int64, C.POINTER(C.c_int64), _dp]
@@ -368,15 +368,28 @@ class Propagator:
             self.last_order = order.value
 
 
-def tile_plan(nspins: int, tile_bits: int) -> list:
-    """The tiled kernel's tile patterns (bit masks, one per pass; the last
-    forms T_n) for an nspins-spin vector and tiles of tile_bits spins."""
+def tiled_select(precision: int, register_bits: int = 0) -> None:
+    """The tiled kernel's schedule for a precision: register bits per thread
+    (FP64 3 or 4, mixed 4 or 5, 0 = default)."""
+    check(load().ss_tiled_select(precision, register_bits))
+
+
+def tile_plan(nspins: int, tile_bits: int, line_bits: int = 0) -> list:
+    """Tile patterns (bit masks, one per pass; the last forms T_n) for an
+    nspins-spin vector and tiles of tile_bits spins that all hold spins
+    0 .. line_bits-1."""
     lib = load()
     n = C.c_int32()
-    check(lib.ss_tile_plan(nspins, tile_bits, C.byref(n), None, 0))
+    check(lib.ss_tile_plan(nspins, tile_bits, line_bits, C.byref(n), None, 0))
     masks = (C.c_uint32 * max(1, n.value))()
-    check(lib.ss_tile_plan(nspins, tile_bits, C.byref(n), masks, n.value))
+    check(lib.ss_tile_plan(nspins, tile_bits, line_bits, C.byref(n), masks, n.value))
     return [int(m) for m in masks[: n.value]]
+
+
+def tiled_plan(nspins: int, precision: int) -> list:
+    """The patterns SS_KERNEL_TILED runs for a precision (12-spin tiles with
+    8-amplitude runs in FP64, 13-spin tiles with 16-amplitude runs mixed)."""
+    return tile_plan(nspins, 12, 3) if precision == abi.FP64 else tile_plan(nspins, 13, 4)
 
 
 def rotation_matrix(axis: Sequence[float], angle: float) -> np.ndarray:

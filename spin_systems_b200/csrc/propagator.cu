@@ -48,13 +48,16 @@ __global__ void k_cheb_init(double2* psi, C2* t0, size_t n, double a0) {
 }
 
 // One order: T_n = 2H^ T_{n-1} - T_{n-2} (T_1 = H^ T_0), written over T_{n-2};
-// psi += (cr + i ci) T_n  (Propagator.cpp:58-72).  The table is prescaled by
-// -2/bound, so the gather already is 2H^ T_{n-1}.  The gather and T_n's
-// formation are FP64; C2 = float2 stores the mixed path's T vectors in FP32.
+// psi += c_n T_n (+ c_{n-1} T_{n-1}: psi is read and written every second
+// order, taking both terms at once, as `psi_terms` = 0, 1, 2 says)
+// (Propagator.cpp:58-72).  The table is prescaled by -2/bound, so the gather
+// already is 2H^ T_{n-1}.  The gather and T_n's formation are FP64;
+// C2 = float2 stores the mixed path's T vectors in FP32.
 template <typename C2>
 __global__ void k_cheb_order(const HamTerms* __restrict__ t, const double* __restrict__ diag,
                              const C2* __restrict__ cur, C2* prev, double2* psi,
-                             size_t n, int first, double cr, double ci) {
+                             size_t n, int first, double cr, double ci, int psi_terms, double pr,
+                             double pi) {
   const size_t k = blockIdx.x * size_t{blockDim.x} + threadIdx.x;
   if (k >= n) return;
   const double2 h = ham_gather(t, diag, cur, k);
@@ -66,9 +69,15 @@ __global__ void k_cheb_order(const HamTerms* __restrict__ t, const double* __res
     tn = make_double2(h.x - q.x, h.y - q.y);
   }
   prev[k] = narrow<C2>(tn.x, tn.y);
+  if (psi_terms == 0) return;
   double2 p = psi[k];
   p.x += cr * tn.x - ci * tn.y;
   p.y += cr * tn.y + ci * tn.x;
+  if (psi_terms == 2) {
+    const C2 o = cur[k];
+    p.x += pr * o.x - pi * o.y;
+    p.y += pr * o.y + pi * o.x;
+  }
   psi[k] = p;
 }
 
@@ -130,8 +139,10 @@ void evolve(ss_ham* h, ss_state* psi, const std::vector<double>& weights, double
   ensure_evolve_scratch(e, h->nspins);
   const bool tiled = kernel != SS_KERNEL_GATHER;
   const void* passes = nullptr;
+  int variant = 0;  // the tiled family's schedule: its kernels differ per variant
   if (tiled) {
     passes = tiled_prepare(h, scale, precision, kernel);
+    variant = tile_variant(precision, kernel);
     ensure_part_scratch(e, h->nspins);
   }
   const bool mixed = precision == SS_PRECISION_MIXED;
@@ -151,16 +162,21 @@ void evolve(ss_ham* h, ss_state* psi, const std::vector<double>& weights, double
     for (size_t order = 1; order < ncoef; ++order) {
       const int first = order == 1 ? 1 : 0;
       const double cr = weights[2 * order], ci = weights[2 * order + 1];
+      const double pr = weights[2 * order - 2], pi = weights[2 * order - 1];
+      // psi takes c_{n-1} T_{n-1} + c_n T_n on even orders, c_n T_n alone on
+      // a final odd order, and nothing on the other odd orders.
+      const int psi_terms = order % 2 == 0 ? 2 : (order + 1 == ncoef ? 1 : 0);
       if (tiled) {
-        tiled_order(h, precision, kernel, cur, prev, e->evolve_part, psi->data, first, cr, ci);
+        tiled_order(h, precision, kernel, cur, prev, e->evolve_part, psi->data, first, cr, ci,
+                    psi_terms, pr, pi);
       } else if (mixed) {
         launch(e, k_cheb_order<float2>, grid, kThreads, 0, h->dev_terms, h->diag,
                static_cast<const float2*>(cur), static_cast<float2*>(prev), psi->data, n, first,
-               cr, ci);
+               cr, ci, psi_terms, pr, pi);
       } else {
         launch(e, k_cheb_order<double2>, grid, kThreads, 0, h->dev_terms, h->diag,
                static_cast<const double2*>(cur), static_cast<double2*>(prev), psi->data, n, first,
-               cr, ci);
+               cr, ci, psi_terms, pr, pi);
       }
       std::swap(cur, prev);
     }
@@ -177,7 +193,7 @@ void evolve(ss_ham* h, ss_state* psi, const std::vector<double>& weights, double
     if (c.terms == h->dev_terms && c.diag == h->diag && c.psi == psi->data &&
         c.t0 == e->evolve_t[0] && c.t1 == e->evolve_t[1] && c.n == n &&
         c.part == (tiled ? e->evolve_part : nullptr) && c.passes == passes &&
-        c.precision == precision && c.kernel == kernel &&
+        c.precision == precision && c.kernel == kernel * 16 + variant &&
         c.autonormalize == int(autonormalize) && c.weights == weights) {
       g = &c;
       break;
@@ -202,7 +218,7 @@ void evolve(ss_ham* h, ss_state* psi, const std::vector<double>& weights, double
     c.n = n;
     c.autonormalize = int(autonormalize);
     c.precision = precision;
-    c.kernel = kernel;
+    c.kernel = kernel * 16 + variant;
     c.weights = weights;
     const int64_t before = e->launches.load();
     cudaGraph_t graph = nullptr;

@@ -19,21 +19,28 @@
 // the reference's recurrence (src/core/Propagator.cpp:58-72) and its
 // Hamiltonian (src/core/Hamiltonian.cpp:95-127) in one sweep per pass.
 //
+// The last pass holds T_{n-1} (its tile) and forms T_n, so psi is read and
+// written every second order only, taking c_{n-1} T_{n-1} + c_n T_n at once.
+//
 // DRAM traffic per amplitude-order with P passes: T_{n-1} once per pass,
 // the partial written by the first pass, read and written by the middle
-// ones, read by the last, and the last pass's diagonal, T_{n-2}, T_n and psi:
-//   FP64  (16 B amplitudes):  16 P + 32 (P - 1) + 8 + 32 + 32  = 48 P + 40 B
-//   mixed ( 8 B amplitudes):   8 P + 16 (P - 1) + 8 + 16 + 32  = 24 P + 40 B
+// ones, read by the last, and the last pass's diagonal, T_{n-2}, T_n and
+// (every second order) psi:
+//   FP64  (16 B amplitudes):  16 P + 32 (P - 1) + 8 + 32 + 16  = 48 P + 24 B
+//   mixed ( 8 B amplitudes):   8 P + 16 (P - 1) + 8 + 16 + 16  = 24 P + 24 B
 // against the single-sweep 80 / 56 B (+8 B of diagonal) that needs every
-// partner on chip at once.  At L = 24 P = 6 (a lower bound for tiles of
-// 12-14 spins that keep low bits for coalescing).
+// partner on chip at once.  Every tile keeps the lowest spins, so each copy
+// moves whole 128-byte lines (8 FP64 or 16 FP32 amplitudes): at L = 24 that
+// takes P = 7.
 //
 // Mixed precision: T vectors and the partial sums are FP32 and the couplings
 // are applied as FP32 numbers; the diagonal, T_n's formation, the series
 // weights and psi are FP64 (the batched engine's scheme).
 #include <algorithm>
+#include <atomic>
 #include <map>
 #include <mutex>
+#include <tuple>
 #include <utility>
 
 #include "batch_kernel.cuh"
@@ -67,6 +74,7 @@ struct PassDev {
   int pad_;
   uint32_t jmask[kMaxLayouts];   // layout g: tile-local spins j with a partner block
   uint32_t rmask[kMaxLayouts];   // layout g: register pairs (p * R + q) with a coefficient
+  uint32_t active;               // bit g: layout g applies something (the last always runs)
   double cff[kMaxTile * kMaxTile];  // [i * B + j], i < j: scale (jx + jy) / 4
   double cfb[kMaxTile * kMaxTile];  // scale (jx - jy) / 4
   double ccx[kMaxTile];             // scale hx / 2
@@ -81,8 +89,10 @@ struct OrderArgs {
   const double* diag;   // sigma_z diagonal, unscaled
   double dscale;        // scale of the diagonal
   double cr, ci;        // series weight c_n
+  double pr, pi;        // series weight c_{n-1}
   uint32_t ntiles;
   int first;            // order 1: T_1 = H^ T_0
+  int psi_terms;        // 0: psi untouched; 1: psi += c_n T_n; 2: also + c_{n-1} T_{n-1}
 };
 
 // ------------------------------------------------------------------ host: plan
@@ -193,35 +203,25 @@ int low_run(uint32_t m) {
   return r;
 }
 
-std::vector<uint32_t> make_plan(int L, int B) {
+// Tiles of B spins that all hold spins 0 .. u-1 (so every copy of a tile
+// moves runs of 2^u consecutive amplitudes), as few as the search finds.
+std::vector<uint32_t> make_plan(int L, int B, int u) {
   if (L <= B) return {L >= 32 ? ~0u : (1u << L) - 1u};
-  std::vector<uint32_t> best = group_cover(L, B, 0);
-  int best_u = 0;
-  // Prefer fewer passes, then more low bits in every tile (longer contiguous
-  // runs per copy).
-  for (int u = std::min(3, B - 2); u >= 0; --u) {
-    const int n = L - u, c = B - u;
-    std::vector<uint32_t> g = group_cover(L, B, u);
-    if (g.size() < best.size() || (g.size() == best.size() && u > best_u)) {
-      best = g;
-      best_u = u;
+  u = std::max(0, std::min(u, B - 2));
+  std::vector<uint32_t> best = group_cover(L, B, u);
+  const int n = L - u, c = B - u;
+  const int r = (n - 1 + c - 2) / (c - 1);  // tiles per spin, at least
+  const int lb = std::max(2, (n * r + c - 1) / c);
+  for (int P = lb; P < static_cast<int>(best.size()); ++P) {
+    std::vector<uint32_t> found;
+    bool ok = false;
+    for (uint64_t seed = 1; seed <= 8 && !ok; ++seed) {
+      ok = search_cover(L, B, u, P, seed * 0x9E3779B97F4A7C15ULL + uint64_t(L * 64 + B), 60000,
+                        &found);
     }
-    const int r = (n - 1 + c - 2) / (c - 1);  // tiles per spin, at least
-    const int lb = std::max(2, (n * r + c - 1) / c);
-    for (int P = lb; P < static_cast<int>(best.size()) ||
-                     (P == static_cast<int>(best.size()) && u > best_u);
-         ++P) {
-      std::vector<uint32_t> found;
-      bool ok = false;
-      for (uint64_t seed = 1; seed <= 8 && !ok; ++seed) {
-        ok = search_cover(L, B, u, P, seed * 0x9E3779B97F4A7C15ULL + uint64_t(L * 64 + B),
-                          60000, &found);
-      }
-      if (ok) {
-        best = found;
-        best_u = u;
-        break;
-      }
+    if (ok) {
+      best = found;
+      break;
     }
   }
   // The kernel's tiles hold exactly B spins: top up smaller ones with the
@@ -257,6 +257,15 @@ __device__ __forceinline__ void cp_async(C2* dst, const C2* src) {
   }
 }
 
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
+// Waits until at most the most recently committed group is in flight.
+__device__ __forceinline__ void cp_async_wait_prior() {
+  asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+}
+
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
@@ -267,9 +276,21 @@ struct Tile {
   using C2 = typename Cplx<Real>::T;
   static constexpr int NT = Gm::NT, NA = Gm::NA, G = Gm::G;
   static constexpr uint32_t NP = Padded<B, R>::N;
+  // Two T_{n-1} tile buffers (the next tile's copy lands while this one is
+  // worked on), the partial sums between layouts, the pass's coefficients.
   static constexpr size_t kSmem =
-      2 * NP * sizeof(C2) + (2 * B * B + 2 * B) * sizeof(Real) + 2 * NA * sizeof(uint32_t);
+      3 * NP * sizeof(C2) + (2 * B * B + 2 * B) * sizeof(Real) + 2 * NA * sizeof(uint32_t);
   static_assert(G <= kMaxLayouts && B <= kMaxTile, "tile too wide");
+};
+
+// The pass's per-layout masks and tile-index bits, copied to shared memory
+// once per launch (they are read in every tile's layouts).
+struct PassMeta {
+  uint32_t jmask[kMaxLayouts];
+  uint32_t rmask[kMaxLayouts];
+  uint32_t active;
+  int nouter;
+  uint32_t outer_pos[kMaxSpins];
 };
 
 // Shared-memory view of one CTA.
@@ -284,16 +305,39 @@ struct TileSmem {
   const Real* ccy;
 };
 
+// The couplings (b + p, j), p < R, from one partner block held in registers:
+// slot x of the block (amplitude k ^ 2^j with register bits x) feeds the
+// thread's slot x ^ 2^p with c1[p] when that slot's bit p is set, c0[p] when
+// it is clear.  MODE 1 keeps only the clear targets, MODE 2 only the set ones
+// (the other half multiplies a zero coefficient when there is no |dd><uu|
+// channel and bit j is the same across the warp).
+template <int R, int MODE, typename C2, typename Real, int NA>
+__device__ __forceinline__ void block_apply(C2 (&acc)[NA], const C2 (&v)[NA], const Real (&c0)[R],
+                                            const Real (&c1)[R]) {
+#pragma unroll
+  for (int x = 0; x < NA; ++x) {
+#pragma unroll
+    for (int p = 0; p < R; ++p) {
+      const int dst = x ^ (1 << p);
+      const bool set = ((dst >> p) & 1) != 0;
+      if ((MODE == 1 && set) || (MODE == 2 && !set)) continue;
+      const Real c = set ? c1[p] : c0[p];
+      acc[dst].x += c * v[x].x;
+      acc[dst].y += c * v[x].y;
+    }
+  }
+}
+
 // One register-blocked layout over the tile (the batched engine's
 // layout_pass, restricted to the pass's couplings): own[] receives the
-// thread's T_{n-1} amplitudes, acc[] the partial sums (from shared memory, or
-// zero for the first layout of a first pass).
-template <typename Real, int B, int R, int g, bool ACC_IN>
+// thread's T_{n-1} amplitudes, acc[] the partial sums (from shared memory when
+// `acc_in`, else zero).
+template <typename Real, int B, int R, int g>
 __device__ __forceinline__ void tile_layout(const TileSmem<Real>& sm,
                                             typename Cplx<Real>::T (&acc)[Geo<B, R>::NA],
                                             typename Cplx<Real>::T (&own)[Geo<B, R>::NA],
                                             uint32_t t, uint32_t jmask, uint32_t rmask,
-                                            bool has_trans, bool has_fb) {
+                                            bool acc_in, bool has_trans, bool has_fb) {
   using Gm = Geo<B, R>;
   using C2 = typename Cplx<Real>::T;
   constexpr int b = Gm::base(g);
@@ -302,7 +346,7 @@ __device__ __forceinline__ void tile_layout(const TileSmem<Real>& sm,
   const C2* mine = sm.buf + pad<R>(kb);
 #pragma unroll
   for (int a = 0; a < NA; ++a) own[a] = mine[pad<R>(uint32_t(a) << b)];
-  if constexpr (ACC_IN) {
+  if (acc_in) {
     const C2* pp = sm.acc + pad<R>(kb);
 #pragma unroll
     for (int a = 0; a < NA; ++a) acc[a] = pp[pad<R>(uint32_t(a) << b)];
@@ -354,46 +398,80 @@ __device__ __forceinline__ void tile_layout(const TileSmem<Real>& sm,
   }
 
   // Couplings (b + p, j) with j above the group, one partner block per j
-  // that has a coupling in this pass.
+  // that has a coupling in this pass.  The first half of the next block is
+  // loaded before this block's products, so its latency overlaps them.
+  constexpr int H = NA / 2;
+  if (jmask == 0u) return;
+  int j = __ffs(jmask) - 1;
+  jmask &= jmask - 1u;
+  C2 v[NA];
+#pragma unroll
+  for (int x = 0; x < NA; ++x) v[x] = sm.buf[pad<R>(kb ^ (1u << j)) + pad<R>(uint32_t(x) << b)];
 #pragma unroll 1
-  while (jmask != 0u) {
-    const int j = __ffs(jmask) - 1;
-    jmask &= jmask - 1u;
-    const uint32_t m = 1u << j;
-    const bool bj = (kb & m) != 0;
+  for (;;) {
+    const bool bj = ((kb >> j) & 1u) != 0u;
     Real c0[R], c1[R];
 #pragma unroll
     for (int p = 0; p < R; ++p) {
       const bool mine_p = Gm::cross_mine(g, p);
       const Real ff = mine_p ? sm.cff[(b + p) * B + j] : Real(0);
       const Real fb = mine_p ? sm.cfb[(b + p) * B + j] : Real(0);
-      c0[p] = bj ? ff : fb;
-      c1[p] = bj ? fb : ff;
+      c0[p] = bj ? ff : fb;  // register bit clear: aligned iff bit j clear
+      c1[p] = bj ? fb : ff;  // register bit set
     }
-    cross_block<R, b>(acc, sm.buf + pad<R>(kb ^ m), c0, c1, bj, has_fb);
+    const int jn = jmask != 0u ? __ffs(jmask) - 1 : -1;
+    const C2* nb = sm.buf + pad<R>(kb ^ (1u << (jn >= 0 ? jn : j)));
+    C2 w[H];
+#pragma unroll
+    for (int x = 0; x < H; ++x) w[x] = nb[pad<R>(uint32_t(x) << b)];
+    if (!has_fb && __all_sync(0xffffffffu, bj)) {
+      block_apply<R, 1>(acc, v, c0, c1);
+    } else if (!has_fb && __all_sync(0xffffffffu, !bj)) {
+      block_apply<R, 2>(acc, v, c0, c1);
+    } else {
+      block_apply<R, 0>(acc, v, c0, c1);
+    }
+    if (jn < 0) break;
+    jmask &= jmask - 1u;
+    j = jn;
+#pragma unroll
+    for (int x = 0; x < H; ++x) v[x] = w[x];
+#pragma unroll
+    for (int x = H; x < NA; ++x) v[x] = nb[pad<R>(uint32_t(x) << b)];
   }
 }
 
-template <typename Real, int B, int R, int g, bool ACC0>
-__device__ __forceinline__ void tile_front(const TileSmem<Real>& sm, const PassDev* pd, uint32_t t,
-                                           bool has_trans, bool has_fb) {
+// Layouts 0 .. G-2 that apply something in this pass, each handing its
+// partial sums to the next through shared memory.  `acc_in`: the partial sums
+// in shared memory already hold something (the previous passes' sums, or an
+// earlier layout's).
+template <typename Real, int B, int R, int g>
+__device__ __forceinline__ void tile_front(const TileSmem<Real>& sm, const PassMeta* pd, uint32_t t,
+                                           bool acc_in, bool has_trans, bool has_fb) {
   using Gm = Geo<B, R>;
   if constexpr (g < Gm::G - 1) {
-    using C2 = typename Cplx<Real>::T;
-    C2 acc[Gm::NA], own[Gm::NA];
-    tile_layout<Real, B, R, g, (g > 0 || ACC0)>(sm, acc, own, t, pd->jmask[g], pd->rmask[g],
-                                                 has_trans, has_fb);
-    constexpr int b = Gm::base(g);
-    const uint32_t kb = ((t >> b) << (b + R)) | (t & ((1u << b) - 1u));
-    C2* pp = sm.acc + pad<R>(kb);
+    if ((pd->active >> g) & 1u) {
+      using C2 = typename Cplx<Real>::T;
+      C2 acc[Gm::NA], own[Gm::NA];
+      tile_layout<Real, B, R, g>(sm, acc, own, t, pd->jmask[g], pd->rmask[g], acc_in, has_trans,
+                                 has_fb);
+      constexpr int b = Gm::base(g);
+      const uint32_t kb = ((t >> b) << (b + R)) | (t & ((1u << b) - 1u));
+      C2* pp = sm.acc + pad<R>(kb);
 #pragma unroll
-    for (int a = 0; a < Gm::NA; ++a) pp[pad<R>(uint32_t(a) << b)] = acc[a];
-    __syncthreads();
-    tile_front<Real, B, R, g + 1, ACC0>(sm, pd, t, has_trans, has_fb);
+      for (int a = 0; a < Gm::NA; ++a) pp[pad<R>(uint32_t(a) << b)] = acc[a];
+      __syncthreads();
+      acc_in = true;
+    }
+    tile_front<Real, B, R, g + 1>(sm, pd, t, acc_in, has_trans, has_fb);
   }
 }
 
-// One pass of one Chebyshev order over every tile (persistent CTAs).
+// One pass of one Chebyshev order over every tile (persistent CTAs).  The
+// CTA's tiles are taken in turn; the copy of the next tile's T_{n-1} is
+// issued before this tile is worked on, and (middle and last passes) the
+// next tile's partial sums are copied into the accumulator buffer as soon as
+// the last layout has read this tile's.
 template <typename Real, int B, int R, int KIND>
 __global__ void __launch_bounds__(Geo<B, R>::NT, 1)
     k_tile(const PassDev* __restrict__ pd, OrderArgs a) {
@@ -405,8 +483,8 @@ __global__ void __launch_bounds__(Geo<B, R>::NT, 1)
   constexpr bool kAccIn = KIND == PASS_MID || KIND == PASS_LAST;
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C2* buf = reinterpret_cast<C2*>(smem_raw);
-  C2* accb = buf + NP;
+  C2* bufs = reinterpret_cast<C2*>(smem_raw);  // [2][NP]
+  C2* accb = bufs + 2 * NP;
   Real* cff = reinterpret_cast<Real*>(accb + NP);
   Real* cfb = cff + B * B;
   Real* ccx = cfb + B * B;
@@ -414,10 +492,20 @@ __global__ void __launch_bounds__(Geo<B, R>::NT, 1)
   uint32_t* dep_ld = reinterpret_cast<uint32_t*>(ccy + B);
   uint32_t* dep_rg = dep_ld + NA;
 
+  __shared__ PassMeta meta;
   const uint32_t t = threadIdx.x;
   for (int i = t; i < B * B; i += NT) {
     cff[i] = Real(pd->cff[i]);
     cfb[i] = Real(pd->cfb[i]);
+  }
+  if (t < kMaxLayouts) {
+    meta.jmask[t] = pd->jmask[t];
+    meta.rmask[t] = pd->rmask[t];
+  }
+  if (t < kMaxSpins) meta.outer_pos[t] = pd->outer_pos[t];
+  if (t == 0) {
+    meta.active = pd->active;
+    meta.nouter = pd->nouter;
   }
   if (t < B) {
     ccx[t] = Real(pd->ccx[t]);
@@ -433,28 +521,46 @@ __global__ void __launch_bounds__(Geo<B, R>::NT, 1)
   const uint32_t kb_last = ((t >> bl) << (bl + R)) | (t & ((1u << bl) - 1u));
   const uint32_t dep_kb = deposit(kb_last, pd->tile_pos, B);
   const bool has_trans = pd->has_trans != 0, has_fb = pd->has_fb != 0;
-  const TileSmem<Real> sm{buf, accb, cff, cfb, ccx, ccy};
   __syncthreads();
 
   const C2* cur = static_cast<const C2*>(a.cur);
   C2* part = static_cast<C2*>(a.part);
   C2* prev = static_cast<C2*>(a.prev);
-  for (uint32_t tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
-    const uint32_t base = deposit(tile, pd->outer_pos, pd->nouter);
+  auto copy_tile = [&](C2* dst, const C2* src, uint32_t base) {
 #pragma unroll
     for (int m = 0; m < NA; ++m) {
       const uint32_t s = t + uint32_t(m) * NT;
-      const size_t gi = base | dep_t | dep_ld[m];
-      cp_async(buf + pad<R>(s), cur + gi);
-      if constexpr (kAccIn) cp_async(accb + pad<R>(s), part + gi);
+      cp_async(dst + pad<R>(s), src + (base | dep_t | dep_ld[m]));
     }
-    cp_async_wait_all();
+  };
+  const PassMeta* pm = &meta;
+  uint32_t tile = blockIdx.x;
+  if (tile < a.ntiles) {
+    const uint32_t base = deposit(tile, pm->outer_pos, pm->nouter);
+    copy_tile(bufs, cur, base);
+    if constexpr (kAccIn) copy_tile(accb, part, base);
+  }
+  cp_async_commit();
+  for (int it = 0; tile < a.ntiles; ++it, tile += gridDim.x) {
+    const uint32_t base = deposit(tile, pm->outer_pos, pm->nouter);
+    const uint32_t next = tile + gridDim.x;
+    const uint32_t next_base = next < a.ntiles ? deposit(next, pm->outer_pos, pm->nouter) : 0u;
+    if (next < a.ntiles) copy_tile(bufs + ((it + 1) & 1) * NP, cur, next_base);
+    cp_async_commit();
+    cp_async_wait_prior();  // every copy but the one just issued has landed
     __syncthreads();
 
-    tile_front<Real, B, R, 0, kAccIn>(sm, pd, t, has_trans, has_fb);
+    const TileSmem<Real> sm{bufs + (it & 1) * NP, accb, cff, cfb, ccx, ccy};
+    tile_front<Real, B, R, 0>(sm, pm, t, kAccIn, has_trans, has_fb);
     C2 acc[NA], own[NA];
-    tile_layout<Real, B, R, G - 1, true>(sm, acc, own, t, pd->jmask[G - 1], pd->rmask[G - 1],
-                                         has_trans, has_fb);
+    const bool acc_in = kAccIn || (pm->active & ((1u << (G - 1)) - 1u)) != 0u;
+    tile_layout<Real, B, R, G - 1>(sm, acc, own, t, pm->jmask[G - 1], pm->rmask[G - 1], acc_in,
+                                   has_trans, has_fb);
+    if constexpr (kAccIn) {
+      __syncthreads();  // every thread has read its partial sums
+      if (next < a.ntiles) copy_tile(accb, part, next_base);
+      cp_async_commit();
+    }
     const size_t g0 = base | dep_kb;
     if constexpr (KIND == PASS_FIRST || KIND == PASS_MID) {
 #pragma unroll
@@ -479,14 +585,22 @@ __global__ void __launch_bounds__(Geo<B, R>::NT, 1)
         tn.x = Real(hx);
         tn.y = Real(hy);
         prev[gi] = tn;
-        double2 p = a.psi[gi];
-        p.x += cr * hx - ci * hy;
-        p.y += cr * hy + ci * hx;
-        a.psi[gi] = p;
+        if (a.psi_terms != 0) {
+          double2 p = a.psi[gi];
+          p.x += cr * hx - ci * hy;
+          p.y += cr * hy + ci * hx;
+          if (a.psi_terms == 2) {
+            const double ox = double(own[x].x), oy = double(own[x].y);
+            p.x += a.pr * ox - a.pi * oy;
+            p.y += a.pr * oy + a.pi * ox;
+          }
+          a.psi[gi] = p;
+        }
       }
     }
-    __syncthreads();  // every read of this tile's buffers is done
+    __syncthreads();  // this tile's buffer is free for the copy after next
   }
+  cp_async_wait_all();
 }
 
 // -------------------------------------------------------------- host glue
@@ -495,6 +609,7 @@ using Kernel = void (*)(const PassDev*, OrderArgs);
 
 struct Family {
   int B = 0, R = 0, nt = 0;
+  int line_bits = 0;  // every tile holds spins 0 .. line_bits-1: 128-byte runs
   size_t smem = 0;
   Kernel k[4] = {nullptr, nullptr, nullptr, nullptr};
 };
@@ -506,6 +621,7 @@ Family family() {
   f.B = B;
   f.R = R;
   f.nt = T::NT;
+  f.line_bits = sizeof(typename T::C2) == 16 ? 3 : 4;
   f.smem = T::kSmem;
   f.k[PASS_FIRST] = k_tile<Real, B, R, PASS_FIRST>;
   f.k[PASS_MID] = k_tile<Real, B, R, PASS_MID>;
@@ -514,14 +630,22 @@ Family family() {
   return f;
 }
 
+// Register bits per thread of the tiled kernel, per precision (a schedule
+// choice: fewer bits, more threads per tile; ss_tiled_select changes it).
+std::atomic<int> g_register_bits[2] = {3, 4};
+
 const Family& family_for(int precision, int kernel) {
-  static const Family f64 = family<double, 12, 4>();
-  static const Family f32 = family<float, 13, 4>();
+  static const Family f64r3 = family<double, 12, 3>();
+  static const Family f64r4 = family<double, 12, 4>();
+  static const Family f32r4 = family<float, 13, 4>();
+  static const Family f32r5 = family<float, 13, 5>();
   static const Family s64 = family<double, 8, 3>();
   static const Family s32 = family<float, 8, 3>();
   const bool mixed = precision == SS_PRECISION_MIXED;
   if (kernel == SS_KERNEL_TILED_SMALL) return mixed ? s32 : s64;
-  return mixed ? f32 : f64;
+  const int r = g_register_bits[mixed ? 1 : 0].load();
+  if (mixed) return r == 5 ? f32r5 : f32r4;
+  return r == 4 ? f64r4 : f64r3;
 }
 
 // Builds pass p's table for layouts of R register bits.
@@ -588,48 +712,62 @@ void fill_pass(PassDev* pd, int L, int B, int R, uint32_t tile, const std::vecto
           pd->rmask[g] |= 1u << (p * R + q);
         }
       }
+      if (first_layout(b + p) == g && (pd->ccx[b + p] != 0.0 || pd->ccy[b + p] != 0.0)) {
+        pd->active |= 1u << g;
+      }
       if (!cross_mine(g, p)) continue;
       for (int j = b + R; j < B; ++j) {
         const int i = b + p;
         if (pd->cff[i * B + j] != 0.0 || pd->cfb[i * B + j] != 0.0) pd->jmask[g] |= 1u << j;
       }
     }
+    if (pd->rmask[g] != 0u || pd->jmask[g] != 0u) pd->active |= 1u << g;
   }
+  pd->active |= 1u << (G - 1);
 }
 
 }  // namespace tiled
 
 // Per-Hamiltonian device tables of the tiled kernel.
 struct TiledTables {
-  int precision = -1, kernel = -1, nspins = 0;
+  int precision = -1, kernel = -1, nspins = 0, register_bits = 0;
   double scale = 0.0;
   bool valid = false;
   std::vector<uint32_t> plan;
   tiled::PassDev* dev = nullptr;
 };
 
-std::vector<uint32_t> tile_plan(int nspins, int tile_bits) {
+std::vector<uint32_t> tile_plan(int nspins, int tile_bits, int line_bits) {
   static std::mutex mu;
-  static std::map<std::pair<int, int>, std::vector<uint32_t>> cache;
+  static std::map<std::tuple<int, int, int>, std::vector<uint32_t>> cache;
   require(nspins >= 1 && nspins <= kMaxSpins, SS_ERR_OUT_OF_RANGE,
           "number of spins must be in [1, kMaxSpins]");
   require(tile_bits >= 2 && tile_bits <= tiled::kMaxTile, SS_ERR_INVALID_ARGUMENT,
           "tile width out of range");
+  require(line_bits >= 0 && line_bits <= 8, SS_ERR_INVALID_ARGUMENT, "line bits out of range");
   std::lock_guard<std::mutex> lock(mu);
-  auto it = cache.find({nspins, tile_bits});
+  auto it = cache.find({nspins, tile_bits, line_bits});
   if (it != cache.end()) return it->second;
-  std::vector<uint32_t> p = tiled::make_plan(nspins, tile_bits);
+  std::vector<uint32_t> p = tiled::make_plan(nspins, tile_bits, line_bits);
   require(tiled::covers(nspins, p), SS_ERR_RUNTIME, "tile plan does not cover every pair");
   for (uint32_t m : p) {
     require(__builtin_popcount(m) == std::min(nspins, tile_bits), SS_ERR_RUNTIME,
             "tile plan has a tile of the wrong width");
   }
-  cache.emplace(std::make_pair(nspins, tile_bits), p);
+  cache.emplace(std::make_tuple(nspins, tile_bits, line_bits), p);
   return p;
 }
 
 int tile_bits_for(int precision, int kernel) {
   return tiled::family_for(precision, kernel).B;
+}
+
+int tile_variant(int precision, int kernel) {
+  return tiled::family_for(precision, kernel).R;
+}
+
+int tile_line_bits(int precision, int kernel) {
+  return tiled::family_for(precision, kernel).line_bits;
 }
 
 void tiled_release(ss_ham* h) {
@@ -658,8 +796,9 @@ const void* tiled_prepare(ss_ham* h, double scale, int precision, int kernel) {
   }
   if (h->tiled == nullptr) h->tiled = new TiledTables;
   TiledTables* tt = h->tiled;
-  if (tt->precision != precision || tt->kernel != kernel || tt->nspins != L) {
-    std::vector<uint32_t> plan = tile_plan(L, f.B);
+  if (tt->precision != precision || tt->kernel != kernel || tt->nspins != L ||
+      tt->register_bits != f.R) {
+    std::vector<uint32_t> plan = tile_plan(L, f.B, f.line_bits);
     if (tt->dev == nullptr || plan.size() > tt->plan.size()) {
       sync(h->engine);
       cudaFree(tt->dev);
@@ -670,19 +809,21 @@ const void* tiled_prepare(ss_ham* h, double scale, int precision, int kernel) {
     tt->precision = precision;
     tt->kernel = kernel;
     tt->nspins = L;
+    tt->register_bits = f.R;
     tt->valid = false;
   }
   if (!tt->valid || tt->scale != scale || !h->tiled_terms_valid) {
     const int P = static_cast<int>(tt->plan.size());
-    // Each coupling to the pass holding both spins that has the fewest so
-    // far; each field to the first pass holding its spin.
-    std::vector<int> owner(h->pairs.size(), -1), load(P, 0);
+    // Each coupling to the last pass holding both spins (a pass's cost grows
+    // with the partner blocks it reads, so concentrating the couplings on
+    // few passes leaves the others fewer blocks); each field to the first
+    // pass holding its spin.
+    std::vector<int> owner(h->pairs.size(), -1);
     for (size_t i = 0; i < h->pairs.size(); ++i) {
       const uint32_t m = (1u << h->pairs[i].lo) | (1u << h->pairs[i].hi);
       for (int p = 0; p < P; ++p) {
-        if ((tt->plan[p] & m) == m && (owner[i] < 0 || load[p] < load[owner[i]])) owner[i] = p;
+        if ((tt->plan[p] & m) == m) owner[i] = p;
       }
-      ++load[owner[i]];
     }
     std::vector<uint32_t> field_owner(L, 0);
     for (int s = 0; s < L; ++s) {
@@ -708,7 +849,8 @@ const void* tiled_prepare(ss_ham* h, double scale, int precision, int kernel) {
 }
 
 void tiled_order(ss_ham* h, int precision, int kernel, const void* cur, void* prev, void* part,
-                 double2* psi, int first, double cr, double ci) {
+                 double2* psi, int first, double cr, double ci, int psi_terms, double pr,
+                 double pi) {
   const tiled::Family& f = tiled::family_for(precision, kernel);
   TiledTables* tt = h->tiled;
   ss_engine* e = h->engine;
@@ -722,7 +864,10 @@ void tiled_order(ss_ham* h, int precision, int kernel, const void* cur, void* pr
   a.dscale = tt->scale;
   a.cr = cr;
   a.ci = ci;
+  a.pr = pr;
+  a.pi = pi;
   a.first = first;
+  a.psi_terms = psi_terms;
   a.ntiles = 1u << (h->nspins - f.B);
   const unsigned int grid = std::min<unsigned int>(a.ntiles, static_cast<unsigned int>(e->sm_count));
   for (int p = 0; p < P; ++p) {
@@ -740,10 +885,24 @@ using namespace ss;
 
 extern "C" {
 
-int ss_tile_plan(int nspins, int tile_bits, int32_t* npass, uint32_t* masks, int32_t cap) {
+int ss_tiled_select(int precision, int register_bits) {
+  return guarded([&] {
+    require(precision == SS_PRECISION_FP64 || precision == SS_PRECISION_MIXED,
+            SS_ERR_INVALID_ARGUMENT, "unknown precision");
+    const int def = precision == SS_PRECISION_MIXED ? 4 : 3;
+    const int r = register_bits == 0 ? def : register_bits;
+    const bool ok = precision == SS_PRECISION_MIXED ? (r == 4 || r == 5) : (r == 3 || r == 4);
+    require(ok, SS_ERR_INVALID_ARGUMENT,
+            "register bits: 3 or 4 for FP64 tiles, 4 or 5 for mixed-precision tiles");
+    tiled::g_register_bits[precision == SS_PRECISION_MIXED ? 1 : 0].store(r);
+  });
+}
+
+int ss_tile_plan(int nspins, int tile_bits, int line_bits, int32_t* npass, uint32_t* masks,
+                 int32_t cap) {
   return guarded([&] {
     require(npass != nullptr, SS_ERR_INVALID_ARGUMENT, "null output");
-    const std::vector<uint32_t> p = tile_plan(nspins, tile_bits);
+    const std::vector<uint32_t> p = tile_plan(nspins, tile_bits, line_bits);
     *npass = static_cast<int32_t>(p.size());
     if (masks != nullptr) {
       require(cap >= static_cast<int32_t>(p.size()), SS_ERR_INVALID_ARGUMENT,

@@ -178,14 +178,14 @@ def plain(args) -> dict:
     terms applied per second, and the mixed result's deviation from FP64 after
     the timed steps.  Then the streaming StateVector kernels at L = 26 (1 GiB
     vectors), which have no partner gathers."""
-    from . import Hamiltonian, Propagator, StateVector, tile_plan
+    from . import Hamiltonian, Propagator, StateVector, tiled_plan, tiled_select
     eng = Engine(0)
     stream, e0, e1 = _events(eng)
     rep = {"order_kernel": {}, "streaming": {}}
-    combos = [("fp64", abi.FP64, "gather", abi.KERNEL_GATHER),
-              ("fp64", abi.FP64, "tiled", abi.KERNEL_TILED),
-              ("mixed", abi.MIXED, "gather", abi.KERNEL_GATHER),
-              ("mixed", abi.MIXED, "tiled", abi.KERNEL_TILED)]
+    combos = [("fp64", abi.FP64, "gather", abi.KERNEL_GATHER, 0),
+              ("mixed", abi.MIXED, "gather", abi.KERNEL_GATHER, 0)]
+    combos += [("fp64", abi.FP64, "tiled", abi.KERNEL_TILED, r) for r in args.fp64_bits]
+    combos += [("mixed", abi.MIXED, "tiled", abi.KERNEL_TILED, r) for r in args.mixed_bits]
     for L in args.sizes:
         spec = workloads.long_propagation(nspins=L, steps=1, every=1, epsilon=1e-7)
         cfg = spec.config()
@@ -195,9 +195,12 @@ def plain(args) -> dict:
         npairs = len(s["pairs"]) // 2
         out = {"pairs": npairs}
         final = {}
-        for pname, prec, kname, kern in combos:
+        for pname, prec, kname, kern, bits in combos:
             if kname in args.skip or (kname == "gather" and L > args.gather_max):
                 continue
+            if kname == "tiled":
+                tiled_select(prec, bits)
+                kname = f"tiled_r{bits}"
             psi = StateVector(eng, L, s["psi0"])
             prop = Propagator(L, 1e-7, prec, kern)
             prop.evolve(ham, abi.REAL, psi, 0.1, 1)          # warm-up, builds the tables
@@ -212,20 +215,22 @@ def plain(args) -> dict:
             r = {"orders": int(orders), "ms_per_order": 1e3 * sec / orders,
                  "effective_gbs": alg * amps * orders / sec / 1e9, "algorithmic_bytes": alg,
                  "pair_terms_per_s": 0.5 * npairs * amps * orders / sec}
-            if kname == "tiled":
-                P = len(tile_plan(L, 12 if prec == abi.FP64 else 13))
+            if kname.startswith("tiled"):
+                P = len(tiled_plan(L, prec))
                 r["passes"] = P
-                r["pass_bytes"] = (48.0 * P + 40.0) if prec == abi.FP64 else (24.0 * P + 40.0)
+                r["pass_bytes"] = (48.0 * P + 24.0) if prec == abi.FP64 else (24.0 * P + 24.0)
                 r["pass_gbs"] = r["pass_bytes"] * amps * orders / sec / 1e9
             final[(pname, kname)] = psi.download()
             out[f"{pname}_{kname}"] = r
             del psi
-        ref = final.get(("fp64", "gather"), final.get(("fp64", "tiled")))
+        ref = final.get(("fp64", "gather"), final.get(("fp64", "tiled_r3")))
         for key, v in final.items():
             if ref is not None and key != ("fp64", "gather"):
                 out[f"{key[0]}_{key[1]}"]["max_dev_vs_fp64"] = float(np.abs(v - ref).max())
         rep["order_kernel"][int(L)] = out
         del ham
+        tiled_select(abi.FP64, 0)
+        tiled_select(abi.MIXED, 0)
         print(json.dumps({int(L): out}), flush=True)
     L = 26
     a = StateVector(eng, L)
@@ -319,6 +324,10 @@ def main(argv=None) -> None:
     pl.add_argument("--sizes", type=int, nargs="+", default=[16, 20, 22, 24])
     pl.add_argument("--steps", type=int, default=2)
     pl.add_argument("--skip", nargs="*", default=[], help="kernel families to leave out")
+    pl.add_argument("--fp64-bits", type=int, nargs="+", default=[3, 4],
+                    help="register bits of the FP64 tiled schedules to time")
+    pl.add_argument("--mixed-bits", type=int, nargs="+", default=[4, 5],
+                    help="register bits of the mixed tiled schedules to time")
     pl.add_argument("--gather-max", type=int, default=30,
                     help="largest L timed with the gather kernel")
     pl.add_argument("--out", default="")

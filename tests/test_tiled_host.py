@@ -19,11 +19,13 @@ def low_run(m: int) -> int:
     return r
 
 
-@pytest.mark.parametrize("tile_bits", [8, 12, 13])
-def test_plans_cover_every_pair_with_full_tiles(tile_bits):
+@pytest.mark.parametrize("tile_bits,line_bits", [(8, 3), (8, 4), (12, 3), (13, 4)])
+def test_plans_cover_every_pair_with_full_tiles(tile_bits, line_bits):
     for L in range(tile_bits, 31):
-        plan = ss.tile_plan(L, tile_bits)
+        plan = ss.tile_plan(L, tile_bits, line_bits)
         assert all(bin(m).count("1") == tile_bits for m in plan)
+        # every tile's copies move runs of 2^line_bits consecutive amplitudes
+        assert all(low_run(m) >= min(line_bits, tile_bits - 2) for m in plan)
         assert all(m < (1 << L) for m in plan)
         for i, j in itertools.combinations(range(L), 2):
             pair = (1 << i) | (1 << j)
@@ -34,19 +36,21 @@ def test_plans_cover_every_pair_with_full_tiles(tile_bits):
 
 
 def test_plans_are_reproducible_and_small():
-    first = {L: ss.tile_plan(L, 12) for L in (18, 20, 22, 24)}
-    again = {L: ss.tile_plan(L, 12) for L in (18, 20, 22, 24)}
+    first = {L: ss.tile_plan(L, 12, 3) for L in (18, 20, 22, 24)}
+    again = {L: ss.tile_plan(L, 12, 3) for L in (18, 20, 22, 24)}
     assert first == again
-    # pass counts at the sizes the propagation workloads use (6 passes at
-    # L = 22-24 is the lower bound for 12-spin tiles that keep a low bit)
-    assert len(first[18]) == 3 and len(first[24]) == 6
-    assert len(ss.tile_plan(24, 13)) == 6
+    # pass counts at the sizes the propagation workloads use: whole 128-byte
+    # runs in every tile cost L = 24 a seventh pass over the bare minimum
+    assert len(first[18]) <= 4 and len(first[24]) == 7
+    assert len(ss.tiled_plan(24, 1)) == 7 and ss.tiled_plan(24, 0) == first[24]
 
 
 def test_plan_arguments_are_checked():
     with pytest.raises(ss.OutOfRangeError):
-        ss.tile_plan(31, 12)
+        ss.tile_plan(31, 12, 3)
     with pytest.raises(ss.InvalidArgumentError):
-        ss.tile_plan(20, 14)
+        ss.tile_plan(20, 14, 3)
     with pytest.raises(ss.InvalidArgumentError):
-        ss.tile_plan(20, 1)
+        ss.tile_plan(20, 1, 0)
+    with pytest.raises(ss.InvalidArgumentError):
+        ss.tile_plan(20, 12, 9)
