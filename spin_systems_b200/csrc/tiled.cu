@@ -247,6 +247,13 @@ __device__ __forceinline__ uint32_t deposit(uint32_t x, const uint32_t* pos, int
   return r;
 }
 
+// Length of the run of tile-local bits that sit on basis bits 0, 1, 2, ...
+__device__ __forceinline__ int low_run_of(const PassDev* pd) {
+  int r = 0;
+  while (r < kMaxTile && pd->tile_pos[r] == static_cast<uint32_t>(r)) ++r;
+  return r;
+}
+
 template <typename C2>
 __device__ __forceinline__ void cp_async(C2* dst, const C2* src) {
   const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(dst));
@@ -255,6 +262,12 @@ __device__ __forceinline__ void cp_async(C2* dst, const C2* src) {
   } else {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(src) : "memory");
   }
+}
+
+// Brings the 128-byte line holding `p` into L2 (no register or shared-memory
+// destination: a later load of the line hits L2 instead of DRAM).
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p));
 }
 
 __device__ __forceinline__ void cp_async_commit() {
@@ -520,6 +533,34 @@ __global__ void __launch_bounds__(Geo<B, R>::NT, 1)
   const uint32_t dep_t = deposit(t, pd->tile_pos, B - R);
   const uint32_t kb_last = ((t >> bl) << (bl + R)) | (t & ((1u << bl) - 1u));
   const uint32_t dep_kb = deposit(kb_last, pd->tile_pos, B);
+  // Runs of 2^U consecutive amplitudes (the tile's low spins), 128 bytes of
+  // T_{n-1}: thread t looks after runs t + i NT; dep_run[i] is where run
+  // starts relative to the tile's base.
+  constexpr int U = sizeof(C2) == 16 ? 3 : 4;
+  constexpr int kRuns = 1 << (B - U);
+  constexpr int kRunsPerThread = (kRuns + NT - 1) / NT;
+  const bool runs_ok = low_run_of(pd) >= U;
+  uint32_t dep_run[kRunsPerThread];
+#pragma unroll
+  for (int i = 0; i < kRunsPerThread; ++i) {
+    const uint32_t r = t + uint32_t(i) * NT;
+    dep_run[i] = r < uint32_t(kRuns) ? deposit(r << U, pd->tile_pos, B) : 0u;
+  }
+  // L2 prefetch of a tile's runs of vector v (elements of type E).
+  auto prefetch_tile = [&](const auto* v, uint32_t base) {
+    if (!runs_ok) return;
+#pragma unroll
+    for (int i = 0; i < kRunsPerThread; ++i) {
+      if (t + uint32_t(i) * NT < uint32_t(kRuns)) {
+        const auto* q = v + (base | dep_run[i]);
+        constexpr int kLines = (sizeof(*q) << U) / 128 > 0 ? (sizeof(*q) << U) / 128 : 1;
+#pragma unroll
+        for (int l = 0; l < kLines; ++l) {
+          prefetch_l2(reinterpret_cast<const char*>(q) + 128 * l);
+        }
+      }
+    }
+  };
   const bool has_trans = pd->has_trans != 0, has_fb = pd->has_fb != 0;
   __syncthreads();
 
@@ -547,6 +588,16 @@ __global__ void __launch_bounds__(Geo<B, R>::NT, 1)
     const uint32_t next_base = next < a.ntiles ? deposit(next, pm->outer_pos, pm->nouter) : 0u;
     if (next < a.ntiles) copy_tile(bufs + ((it + 1) & 1) * NP, cur, next_base);
     cp_async_commit();
+    // Lines this tile's epilogue and the next tile's partial-sum copy will
+    // touch go to L2 now, a tile's work ahead of their use.
+    if constexpr (kAccIn) {
+      if (next < a.ntiles) prefetch_tile(part, next_base);
+    }
+    if constexpr (KIND == PASS_LAST || KIND == PASS_ONLY) {
+      prefetch_tile(a.diag, base);
+      prefetch_tile(prev, base);
+      if (a.psi_terms != 0) prefetch_tile(a.psi, base);
+    }
     cp_async_wait_prior();  // every copy but the one just issued has landed
     __syncthreads();
 
