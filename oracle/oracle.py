@@ -351,6 +351,16 @@ class Ref(_Lib):
         self._check(self.lib.refd_random_state(L, C.c_uint64(seed), _d(out)))
         return out
 
+    def experiment_csv(self, cfg: SsRunConfig, threads: int) -> str:
+        """The reference's runExperiment written by its own writeCsv."""
+        need = C.c_size_t()
+        self._check(self.lib.refd_experiment_csv(C.byref(cfg), threads, None, C.c_size_t(0),
+                                                 C.byref(need)))
+        buf = C.create_string_buffer(need.value + 1)
+        self._check(self.lib.refd_experiment_csv(C.byref(cfg), threads, buf,
+                                                 C.c_size_t(need.value + 1), C.byref(need)))
+        return buf.raw[: need.value].decode()
+
     def run_experiment(self, cfg: SsRunConfig, threads: int):
         p, w = self.shape(cfg)
         times = np.zeros(max(p, 1))

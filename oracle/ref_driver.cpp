@@ -18,6 +18,7 @@
 #include <chrono>
 #include <mutex>
 #include <random>
+#include <sstream>
 
 #include "spinsim/core/Bessel.hpp"
 #include "spinsim/core/Chebyshev.hpp"
@@ -477,6 +478,22 @@ int refd_run_experiment(const ss_run_config* c, int threads, double* times, doub
     std::memcpy(mean, m.data(), sizeof(double) * m.size());
     std::memcpy(sd, s.data(), sizeof(double) * s.size());
     std::memcpy(se, e.data(), sizeof(double) * e.size());
+  });
+}
+
+// runExperiment with LocalRunner(threads), written by the reference's own
+// writeCsv (io/Experiment.cpp:74-97): the bytes `spinsim run` prints.
+// `needed` receives the length; the text goes to buf when cap allows.
+int refd_experiment_csv(const ss_run_config* c, int threads, char* buf, size_t cap,
+                        size_t* needed) {
+  return guarded([&] {
+    const RunConfig cfg = toRunConfig(*c);
+    LocalRunner runner(static_cast<std::size_t>(threads));
+    std::ostringstream out;
+    writeCsv(runExperiment(cfg, runner), out);
+    const std::string text = out.str();
+    *needed = text.size();
+    if (buf != nullptr && cap >= text.size()) std::memcpy(buf, text.data(), text.size());
   });
 }
 

@@ -1,15 +1,25 @@
-// Ensemble layer of the C++ API (reference: src/ensemble/*.cpp): random
-// streams and geometry on the host (bit-for-bit with the reference, since
-// glibc's log/sin/cos and mt19937_64 define the streams), states and their
-// operators on the device, statistics on the host.
+// Ensemble layer of the C++ API: random streams, geometry and disorder on the
+// host, states and their operators on the device, statistics on the host.
+//
+// Restated for bit-exact parity with the reference (their arithmetic and the
+// order of their random draws define geometries, fields and initial states,
+// so those are kept; the code around them is this library's own):
+//   Rng::gaussian              src/ensemble/Rng.cpp:8-23 (Box-Muller, u floored at 1e-15)
+//   prepareInitialState        src/ensemble/Ensemble.cpp:20-45 (re then im per k, then
+//                              one normalisation in index order)
+//   generateDipolarLattice2D   src/ensemble/Ensemble.cpp:60-104 (draw order, rejection
+//                              rule, coupling order and r^3 arithmetic)
+//   Accumulator                src/ensemble/Ensemble.cpp:114-166 (Welford in index
+//                              order, Chan's merge)
 #include <atomic>
 #include <cmath>
 #include <exception>
 #include <format>
-#include <mutex>
 #include <numbers>
+#include <optional>
 #include <stdexcept>
 #include <thread>
+#include <utility>
 
 #include "spinsim/core/Device.hpp"
 #include "spinsim/core/SpinOperators.hpp"
@@ -18,132 +28,151 @@
 #include "spinsim_b200.h"
 
 namespace spinsim {
+namespace {
+
+// Box-Muller on two uniforms: (r cos, r sin) with r = sqrt(-2 ln u).
+std::pair<double, double> boxMuller(double u, double v) {
+  const double r = std::sqrt(-2.0 * std::log(u));
+  const double phase = 2.0 * std::numbers::pi * v;
+  return {r * std::cos(phase), r * std::sin(phase)};
+}
+
+// Scales v to unit norm, the squares summed in index order.
+void normalizeInIndexOrder(double* v, std::size_t n) {
+  double sum = 0.0;
+  for (std::size_t i = 0; i < n; ++i) sum += v[i] * v[i];
+  const double norm = std::sqrt(sum);
+  if (norm == 0.0) throw std::domain_error("cannot normalize a zero state");
+  const double inv = 1.0 / norm;
+  for (std::size_t i = 0; i < n; ++i) v[i] *= inv;
+}
+
+// Product of single-spin states cos(th/2)|up> + e^{i ph} sin(th/2)|down>
+// with th, ph drawn per spin (additive initial state, not in the reference).
+void fillRandomProduct(StateVector& psi, Rng& rng) {
+  const std::size_t L = psi.nspins();
+  std::vector<double> theta(L), phi(L);
+  for (std::size_t s = 0; s < L; ++s) {
+    theta[s] = std::acos(1.0 - 2.0 * rng.uniform());
+    phi[s] = 2.0 * std::numbers::pi * rng.uniform();
+  }
+  double* d = psi.data();
+  for (std::size_t k = 0; k < psi.size(); ++k) {
+    double re = 1.0, im = 0.0;
+    for (std::size_t s = 0; s < L; ++s) {
+      const bool up = (k >> s) & 1u;
+      const double half = 0.5 * theta[s];
+      const double fr = up ? std::cos(half) : std::sin(half) * std::cos(phi[s]);
+      const double fi = up ? 0.0 : std::sin(half) * std::sin(phi[s]);
+      const double nr = re * fr - im * fi;
+      im = re * fi + im * fr;
+      re = nr;
+    }
+    d[2 * k] = re;
+    d[2 * k + 1] = im;
+  }
+  normalizeInIndexOrder(d, 2 * psi.size());
+}
+
+struct Point {
+  double x = 0.0, y = 0.0;
+};
+
+// A spin position uniform in the square [-h, h]^2, redrawn while it lies
+// within `minSep` of an earlier spin in both coordinates.
+Point drawPosition(Rng& rng, double h, double minSep, const std::vector<Point>& placed) {
+  for (;;) {
+    Point p;
+    p.x = h * (2.0 * rng.uniform() - 1.0);
+    p.y = h * (2.0 * rng.uniform() - 1.0);
+    bool clear = true;
+    for (const Point& q : placed) {
+      if (std::abs(p.x - q.x) < minSep && std::abs(p.y - q.y) < minSep) {
+        clear = false;
+        break;
+      }
+    }
+    if (clear) return p;
+  }
+}
+
+}  // namespace
 
 double Rng::gaussian() {
   if (hasSpare_) {
     hasSpare_ = false;
     return spare_;
   }
-  constexpr double kFloor = 1.0e-15;
-  const double u = kFloor + (1.0 - 2.0 * kFloor) * uniform();
+  constexpr double kEdge = 1.0e-15;  // keeps u away from 0 and 1
+  const double u = kEdge + (1.0 - 2.0 * kEdge) * uniform();
   const double v = uniform();
-  const double radius = std::sqrt(-2.0 * std::log(u));
-  const double phase = 2.0 * std::numbers::pi * v;
-  spare_ = radius * std::sin(phase);
+  const auto [first, second] = boxMuller(u, v);
+  spare_ = second;
   hasSpare_ = true;
-  return radius * std::cos(phase);
+  return first;
 }
 
 InitialStateKind parseInitialStateKind(std::string_view name) {
-  if (name == "random") return InitialStateKind::Random;
-  if (name == "up") return InitialStateKind::AllUp;
-  if (name == "down") return InitialStateKind::AllDown;
-  if (name == "basis") return InitialStateKind::BasisState;
-  if (name == "random_product") return InitialStateKind::RandomProduct;
+  static constexpr std::pair<std::string_view, InitialStateKind> kNames[] = {
+      {"random", InitialStateKind::Random},
+      {"up", InitialStateKind::AllUp},
+      {"down", InitialStateKind::AllDown},
+      {"basis", InitialStateKind::BasisState},
+      {"random_product", InitialStateKind::RandomProduct},
+  };
+  for (const auto& [text, kind] : kNames) {
+    if (text == name) return kind;
+  }
   throw std::invalid_argument(std::format(
       "unknown initial state '{}'; expected random, up, down, basis or random_product", name));
 }
 
-namespace {
-
-// Host normalisation in the reference's summation order, so psi0 is
-// bit-identical to the reference's (StateVector.cpp:43-56).
-void normalizeHost(double* v, std::size_t n) {
-  double sum = 0.0;
-  for (std::size_t i = 0; i < n; ++i) sum += v[i] * v[i];
-  const double nrm = std::sqrt(sum);
-  if (nrm == 0.0) throw std::domain_error("cannot normalize a zero state");
-  const double f = 1.0 / nrm;
-  for (std::size_t i = 0; i < n; ++i) v[i] *= f;
-}
-
-}  // namespace
-
 void prepareInitialState(StateVector& psi, InitialStateKind kind, Rng& rng,
                          std::size_t basisIndex) {
   switch (kind) {
-    case InitialStateKind::AllUp: psi.setBasisState(psi.size() - 1); return;
-    case InitialStateKind::AllDown: psi.setBasisState(0); return;
-    case InitialStateKind::BasisState: psi.setBasisState(basisIndex); return;
-    case InitialStateKind::RandomProduct: {
-      const std::size_t L = psi.nspins();
-      std::vector<double> th(L), ph(L);
-      for (std::size_t s = 0; s < L; ++s) {
-        th[s] = std::acos(1.0 - 2.0 * rng.uniform());
-        ph[s] = 2.0 * std::numbers::pi * rng.uniform();
-      }
+    case InitialStateKind::AllUp: psi.setBasisState(psi.size() - 1); break;
+    case InitialStateKind::AllDown: psi.setBasisState(0); break;
+    case InitialStateKind::BasisState: psi.setBasisState(basisIndex); break;
+    case InitialStateKind::RandomProduct: fillRandomProduct(psi, rng); break;
+    case InitialStateKind::Random: {
+      // Complex Gaussian amplitudes, real part first, in index order.
       double* d = psi.data();
-      for (std::size_t k = 0; k < psi.size(); ++k) {
-        double ar = 1.0, ai = 0.0;
-        for (std::size_t s = 0; s < L; ++s) {
-          double fr, fi;
-          if (k & (std::size_t{1} << s)) {
-            fr = std::cos(0.5 * th[s]);
-            fi = 0.0;
-          } else {
-            const double sn = std::sin(0.5 * th[s]);
-            fr = sn * std::cos(ph[s]);
-            fi = sn * std::sin(ph[s]);
-          }
-          const double nr = ar * fr - ai * fi;
-          ai = ar * fi + ai * fr;
-          ar = nr;
-        }
-        d[2 * k] = ar;
-        d[2 * k + 1] = ai;
-      }
-      normalizeHost(d, 2 * psi.size());
-      return;
+      for (std::size_t i = 0; i < 2 * psi.size(); ++i) d[i] = rng.gaussian();
+      normalizeInIndexOrder(d, 2 * psi.size());
+      break;
     }
-    case InitialStateKind::Random: break;
   }
-  double* d = psi.data();
-  for (std::size_t k = 0; k < psi.size(); ++k) {
-    d[2 * k] = rng.gaussian();
-    d[2 * k + 1] = rng.gaussian();
-  }
-  normalizeHost(d, 2 * psi.size());
 }
 
 void prepareReferenceState(const StateVector& psi, Axis axis, StateVector& reference) {
   if (reference.size() != psi.size()) reference = StateVector(psi.nspins());
-  const int a = axis == Axis::X ? SS_AXIS_X : axis == Axis::Y ? SS_AXIS_Y : SS_AXIS_Z;
-  ss_state* out = reference.device();
-  checkStatus(ss_apply_total_spin(a, psi.device(), out));
+  const int code = axis == Axis::X ? SS_AXIS_X : axis == Axis::Y ? SS_AXIS_Y : SS_AXIS_Z;
+  checkStatus(ss_apply_total_spin(code, psi.device(), reference.device()));
   reference.deviceWritten();
 }
 
 std::vector<Coupling> generateDipolarLattice2D(std::size_t nspins, Rng& rng, double scale,
                                                double minSeparation) {
   if (nspins == 0) throw std::invalid_argument("need at least one spin");
-  const double halfWidth = 0.5 * std::sqrt(static_cast<double>(nspins));
-  std::vector<double> x(nspins, 0.0), y(nspins, 0.0);
-  std::vector<Coupling> couplings;
-  couplings.reserve(nspins * (nspins - 1) / 2);
+  // Placement first: spin 0 at the origin, the others drawn in turn (the
+  // draws are the only use of the stream); then every pair (j, i), j < i,
+  // in order of i, with Jz = scale / r^3 and Jx = Jy = -Jz / 2.
+  const double h = 0.5 * std::sqrt(static_cast<double>(nspins));
+  std::vector<Point> placed(1);
+  placed.reserve(nspins);
+  while (placed.size() < nspins) placed.push_back(drawPosition(rng, h, minSeparation, placed));
+  std::vector<Coupling> out;
+  out.reserve(nspins * (nspins - 1) / 2);
   for (std::size_t i = 1; i < nspins; ++i) {
-    double px = 0.0, py = 0.0;
-    for (bool placed = false; !placed;) {
-      px = halfWidth * (2.0 * rng.uniform() - 1.0);
-      py = halfWidth * (2.0 * rng.uniform() - 1.0);
-      placed = true;
-      for (std::size_t j = 0; j < i; ++j) {
-        if (std::abs(px - x[j]) < minSeparation && std::abs(py - y[j]) < minSeparation) {
-          placed = false;
-          break;
-        }
-      }
-    }
-    x[i] = px;
-    y[i] = py;
     for (std::size_t j = 0; j < i; ++j) {
-      const double dx = px - x[j];
-      const double dy = py - y[j];
+      const double dx = placed[i].x - placed[j].x;
+      const double dy = placed[i].y - placed[j].y;
       const double r2 = dx * dx + dy * dy;
       const double jz = scale / (r2 * std::sqrt(r2));
-      couplings.push_back(Coupling{SpinPair{j, i}, -0.5 * jz, -0.5 * jz, jz});
+      out.push_back(Coupling{SpinPair{j, i}, -0.5 * jz, -0.5 * jz, jz});
     }
   }
-  return couplings;
+  return out;
 }
 
 void applyFieldDisorder(Hamiltonian& hamiltonian, Rng& rng, double sigma) {
@@ -154,18 +183,19 @@ void applyFieldDisorder(Hamiltonian& hamiltonian, Rng& rng, double sigma) {
   }
 }
 
+// ------------------------------------------------------------- statistics
+
 Accumulator::Accumulator(std::size_t width) : mean_(width, 0.0), m2_(width, 0.0) {}
 
 void Accumulator::add(std::span<const double> sample) {
   if (sample.size() != mean_.size()) {
     throw std::invalid_argument("sample width does not match the accumulator");
   }
-  ++count_;
-  const double n = static_cast<double>(count_);
-  for (std::size_t k = 0; k < sample.size(); ++k) {
-    const double delta = sample[k] - mean_[k];
-    mean_[k] += delta / n;
-    m2_[k] += delta * (sample[k] - mean_[k]);
+  const double n = static_cast<double>(++count_);
+  for (std::size_t k = 0; k < sample.size(); ++k) {  // Welford per column
+    const double before = mean_[k];
+    mean_[k] = before + (sample[k] - before) / n;
+    m2_[k] += (sample[k] - before) * (sample[k] - mean_[k]);
   }
 }
 
@@ -179,29 +209,31 @@ void Accumulator::merge(const Accumulator& other) {
     return;
   }
   const double na = static_cast<double>(count_), nb = static_cast<double>(other.count_);
-  const double total = na + nb;
-  for (std::size_t k = 0; k < mean_.size(); ++k) {
-    const double delta = other.mean_[k] - mean_[k];
-    mean_[k] += delta * nb / total;
-    m2_[k] += other.m2_[k] + delta * delta * na * nb / total;
+  const double n = na + nb;
+  for (std::size_t k = 0; k < mean_.size(); ++k) {  // Chan et al. pairwise update
+    const double gap = other.mean_[k] - mean_[k];
+    mean_[k] += gap * nb / n;
+    m2_[k] += other.m2_[k] + gap * gap * na * nb / n;
   }
   count_ += other.count_;
 }
 
 std::vector<double> Accumulator::standardDeviation() const {
-  std::vector<double> out(mean_.size(), 0.0);
-  if (count_ < 2) return out;
-  const double denom = static_cast<double>(count_ - 1);
-  for (std::size_t k = 0; k < out.size(); ++k) out[k] = std::sqrt(m2_[k] / denom);
-  return out;
+  std::vector<double> sd(mean_.size(), 0.0);
+  if (count_ > 1) {
+    const double dof = static_cast<double>(count_ - 1);
+    for (std::size_t k = 0; k < sd.size(); ++k) sd[k] = std::sqrt(m2_[k] / dof);
+  }
+  return sd;
 }
 
 std::vector<double> Accumulator::standardError() const {
-  std::vector<double> out = standardDeviation();
-  if (count_ < 2) return out;
-  const double scale = 1.0 / std::sqrt(static_cast<double>(count_));
-  for (double& v : out) v *= scale;
-  return out;
+  std::vector<double> se = standardDeviation();
+  if (count_ > 1) {
+    const double f = 1.0 / std::sqrt(static_cast<double>(count_));
+    for (double& v : se) v *= f;
+  }
+  return se;
 }
 
 void VectorRecorder::record(double time, std::span<const double> values) {
@@ -214,71 +246,99 @@ void VectorRecorder::clear() {
   values_.clear();
 }
 
-LocalRunner::LocalRunner(std::size_t threads)
-    : threads_(threads > 0 ? threads : std::thread::hardware_concurrency()) {
-  if (threads_ == 0) threads_ = 1;
+// ---------------------------------------------------------------- runners
+
+namespace {
+
+// Realisation indices handed out in increasing order to whichever worker
+// asks next; cancel() hands out nothing more.
+class JobQueue {
+ public:
+  explicit JobQueue(std::size_t n) : n_(n) {}
+  std::optional<std::size_t> next() {
+    const std::size_t i = cursor_.fetch_add(1, std::memory_order_relaxed);
+    if (i >= n_ || cancelled_.load(std::memory_order_relaxed)) return std::nullopt;
+    return i;
+  }
+  void cancel() { cancelled_.store(true, std::memory_order_relaxed); }
+
+ private:
+  std::size_t n_;
+  std::atomic<std::size_t> cursor_{0};
+  std::atomic<bool> cancelled_{false};
+};
+
+// Every realisation's rows folded into one Accumulator in index order, so the
+// statistics do not depend on how the realisations were spread over workers.
+EnsembleResult foldInIndexOrder(std::size_t realizations, std::vector<double> times,
+                                std::span<const std::string> columns,
+                                const std::function<std::span<const double>(std::size_t)>& row) {
+  EnsembleResult result;
+  result.times = std::move(times);
+  result.columns.assign(columns.begin(), columns.end());
+  const std::size_t width = result.times.size() * result.columns.size();
+  result.statistics = Accumulator(width);
+  for (std::size_t i = 0; i < realizations; ++i) result.statistics.add(row(i));
+  return result;
 }
+
+}  // namespace
+
+LocalRunner::LocalRunner(std::size_t threads)
+    : threads_(threads > 0 ? threads : std::max(1u, std::thread::hardware_concurrency())) {}
 
 EnsembleResult LocalRunner::run(std::size_t realizations, std::span<const std::string> columns,
                                 const RealizationJob& job) {
   if (realizations == 0) throw std::invalid_argument("an ensemble needs at least one realisation");
-  std::vector<VectorRecorder> per(realizations);
-  std::atomic<std::size_t> next{0};
-  std::mutex failureMutex;
-  std::exception_ptr failure;
-  const std::size_t workers = std::min(threads_, realizations);
+  // Each worker thread drives the device through its own engine and stream
+  // (the core API's per-thread engine).  A failing realisation stops the
+  // hand-out; of the failures, the lowest realisation index is reported, so
+  // the error does not depend on thread timing.
+  std::vector<VectorRecorder> recorders(realizations);
+  std::vector<std::exception_ptr> errors(realizations);
+  JobQueue queue(realizations);
   {
-    std::vector<std::jthread> pool;
-    for (std::size_t w = 0; w < workers; ++w) {
-      pool.emplace_back([&] {
-        for (;;) {
-          const std::size_t index = next.fetch_add(1);
-          if (index >= realizations) return;
+    std::vector<std::jthread> workers;
+    const std::size_t n = std::min(threads_, realizations);
+    workers.reserve(n);
+    for (std::size_t w = 0; w < n; ++w) {
+      workers.emplace_back([&] {
+        while (const auto index = queue.next()) {
           try {
-            job(index, per[index]);
+            job(*index, recorders[*index]);
           } catch (...) {
-            const std::lock_guard lock(failureMutex);
-            if (!failure) failure = std::current_exception();
-            next.store(realizations);
-            return;
+            errors[*index] = std::current_exception();
+            queue.cancel();
           }
         }
       });
     }
   }
-  if (failure) std::rethrow_exception(failure);
-  EnsembleResult result;
-  result.times = per.front().times();
-  result.columns.assign(columns.begin(), columns.end());
-  const std::size_t points = result.times.size();
-  const std::size_t width = points * result.columns.size();
-  result.statistics = Accumulator(width);
-  for (std::size_t i = 0; i < realizations; ++i) {
-    const VectorRecorder& r = per[i];
-    if (r.rows() != points || r.values().size() != width) {
-      throw std::runtime_error(std::format(
-          "realisation {} recorded {} points and {} values; expected {} and {}", i, r.rows(),
-          r.values().size(), points, width));
-    }
-    result.statistics.add(r.values());
+  for (const std::exception_ptr& e : errors) {
+    if (e) std::rethrow_exception(e);
   }
-  return result;
+  const std::size_t points = recorders.front().rows();
+  const std::size_t width = points * columns.size();
+  for (std::size_t i = 0; i < realizations; ++i) {
+    if (recorders[i].rows() != points || recorders[i].values().size() != width) {
+      throw std::runtime_error(std::format(
+          "realisation {} recorded {} points and {} values; expected {} and {}", i,
+          recorders[i].rows(), recorders[i].values().size(), points, width));
+    }
+  }
+  return foldInIndexOrder(realizations, recorders.front().times(), columns,
+                          [&](std::size_t i) { return std::span<const double>(recorders[i].values()); });
 }
 
 EnsembleResult foldRows(std::size_t realizations, const std::vector<double>& times,
                         std::span<const std::string> columns, const std::vector<double>& rows) {
-  EnsembleResult result;
-  result.times = times;
-  result.columns.assign(columns.begin(), columns.end());
-  const std::size_t width = times.size() * result.columns.size();
+  const std::size_t width = times.size() * columns.size();
   if (rows.size() != realizations * width) {
     throw std::runtime_error("batched rows do not match the measurement shape");
   }
-  result.statistics = Accumulator(width);
-  for (std::size_t i = 0; i < realizations; ++i) {
-    result.statistics.add(std::span<const double>(rows.data() + i * width, width));
-  }
-  return result;
+  return foldInIndexOrder(realizations, times, columns, [&](std::size_t i) {
+    return std::span<const double>(rows.data() + i * width, width);
+  });
 }
 
 }  // namespace spinsim

@@ -132,6 +132,14 @@ def main() -> None:
         out[f"exp_{name}_times"], out[f"exp_{name}_mean"] = t, m
         out[f"exp_{name}_sd"], out[f"exp_{name}_se"] = sd, se
 
+    # The same experiments as the reference's own CSV bytes (writeCsv), the
+    # output `spinsim run` must reproduce.
+    csv_text = {}
+    for name, path, count in (("cpmg_l10", ROOT / "configs" / "cpmg_ideal_l10.toml", None),
+                              ("ref_cpmg8z", REFERENCE_TREE / "configs" / "cpmg8z.toml", 3),
+                              ("ref_rabi", REFERENCE_TREE / "configs" / "rabi_szsz.toml", 3)):
+        csv_text[name] = ref.experiment_csv(tomlcfg.load(path, realizations=count).config(), 4)
+
     np.savez_compressed(OUT / "reference_outputs.npz", **out)
     # The reference's example configurations as parsed documents (JSON), so the
     # device runs can be checked against exp_ref_* where the reference tree
@@ -141,6 +149,7 @@ def main() -> None:
     docs = {name: tomllib.loads((REFERENCE_TREE / "configs" / f"{fname}.toml").read_text())
             for name, fname in (("ref_cpmg8z", "cpmg8z"), ("ref_rabi", "rabi_szsz"))}
     (OUT / "reference_configs.json").write_text(json.dumps(docs, indent=1, sort_keys=True))
+    (OUT / "reference_csv.json").write_text(json.dumps(csv_text, indent=1, sort_keys=True))
     print("wrote", sorted(p.name for p in OUT.glob("*.npz")))
 
 

@@ -7,6 +7,7 @@ import csv
 import io
 import json
 import math
+import os
 import subprocess
 from pathlib import Path
 
@@ -18,7 +19,10 @@ from spin_systems_b200 import config as tomlcfg
 ROOT = Path(__file__).resolve().parents[1]
 CLI = ROOT / "spin_systems_b200" / "bin" / "spinsim"
 CONFIGS = sorted((ROOT / "configs").glob("*.toml"))
-REFERENCE_CONFIGS = Path("/root/reference/configs")
+# The reference's source tree, where present (the same variable the oracle's
+# build reads); the tests that need it skip without it.
+_REF_TREE = os.environ.get("SPINSIM_REFERENCE")
+REFERENCE_CONFIGS = Path(_REF_TREE) / "configs" if _REF_TREE else None
 
 MINIMAL = """
 [system]
@@ -72,10 +76,33 @@ def test_configs_validate_and_describe(path):
     assert f"measurements    {spec.measurement_count()} per realization" in d
 
 
-@pytest.mark.skipif(not REFERENCE_CONFIGS.is_dir(), reason="reference tree not present")
+@pytest.mark.skipif(REFERENCE_CONFIGS is None or not REFERENCE_CONFIGS.is_dir(),
+                    reason="SPINSIM_REFERENCE does not name the reference's source tree")
 def test_reference_configs_parse():
     for p in sorted(REFERENCE_CONFIGS.glob("*.toml")):
         assert cli("validate", p).returncode == 0, p
+
+
+def test_describe_text_is_the_references(tmp_path):
+    # apps/spinsim/main.cpp:80-104: one line per field, names padded to 16
+    # columns, {:g} for the floating-point values, observables each after a
+    # space.  (The reference has no random_product state; this build prints
+    # its name.)
+    want = ("spins           10\n"
+            "state space     1024 amplitudes\n"
+            "initial state   random\n"
+            "realizations    20\n"
+            "seed            20240726\n"
+            "geometry        dipolar 2D, per realization\n"
+            "field disorder  0.5\n"
+            "reference axis  x\n"
+            "epsilon         1e-07\n"
+            "measurements    8 per realization\n"
+            "observables     corr:x norm\n")
+    assert cli("describe", ROOT / "configs" / "cpmg_ideal_l10.toml", check=True).stdout == want
+    d = cli("describe", ROOT / "configs" / "long_propagation_l16.toml", check=True).stdout
+    assert "initial state   random_product\n" in d and "epsilon         1e-12\n" in d
+    assert "field disorder  1\n" in d and "geometry        dipolar 2D, per realization\n" in d
 
 
 def test_minimal_config_and_overrides(tmp_path):
@@ -186,3 +213,41 @@ def test_run_mixed_precision_and_output_file(golden, tmp_path):
     header, body = read_csv(out.read_text())
     mean = golden["exp_cpmg_l10_mean"].reshape(len(body), -1)
     assert np.abs(body[:, 1] - mean[:, 0]).max() < 1e-5
+
+
+def csv_diff(got: str, want: str):
+    """(lines, differing fields, largest relative gap of those fields)."""
+    g, w = got.splitlines(), want.splitlines()
+    assert len(g) == len(w) and g[0] == w[0]
+    fields, gap = 0, 0.0
+    for a, b in zip(g[1:], w[1:]):
+        fa, fb = a.split(","), b.split(",")
+        assert len(fa) == len(fb)
+        for x, y in zip(fa, fb):
+            if x != y:
+                fields += 1
+                gap = max(gap, abs(float(x) - float(y)) / max(abs(float(y)), 1e-300))
+    return len(g), fields, gap
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("engine", ["batch", "plain"])
+def test_run_csv_is_the_references_bytes(engine, tmp_path):
+    # `spinsim run` against the reference's own runExperiment + writeCsv
+    # (io/Experiment.cpp:57-97), byte for byte.  The FP64 sums on the device
+    # add the same terms in another order, so a field's 12th significant
+    # digit may round the other way: such fields are counted and bounded by
+    # a relative gap of 1e-10 (the CSV prints 12 digits).
+    want = json.loads((ROOT / "tests" / "golden" / "reference_csv.json").read_text())
+    got = cli("run", ROOT / "configs" / "cpmg_ideal_l10.toml", "--engine", engine,
+              check=True).stdout
+    lines, fields, gap = csv_diff(got, want["cpmg_l10"])
+    assert gap < 1e-10, (fields, gap)
+    assert fields <= 2, fields
+    docs = json.loads((ROOT / "tests" / "golden" / "reference_configs.json").read_text())
+    for name in ("ref_cpmg8z", "ref_rabi"):
+        p = write(tmp_path, dump_toml(docs[name]), f"{name}.toml")
+        got = cli("run", p, "--realizations", "3", "--engine", engine, check=True).stdout
+        lines, fields, gap = csv_diff(got, want[name])
+        assert gap < 1e-10, (name, fields, gap)
+        assert fields <= lines // 10, (name, fields, lines)
