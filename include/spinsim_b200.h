@@ -379,6 +379,12 @@ int ss_batch_io_bytes(const ss_batch* batch, int64_t* h2d, int64_t* d2h);
    Either output may be NULL. */
 int ss_batch_precisions(const ss_batch* batch, int32_t* precision,
                         double* amplitude_orders);
+/* No counterpart in the reference: per realisation, in index order, the
+   coherent error mixed precision would accumulate -- Chebyshev orders (both
+   vectors) times the FP32 rounding residuals of the coefficients the kernel
+   leaves uncorrected, in the expansion's scaled units -- whatever precision
+   it runs in. */
+int ss_batch_error_estimates(const ss_batch* batch, double* estimate);
 
 /* ------------------------------------------------------------- autotuner
  * No counterpart in the reference (its CPU kernels have one schedule).

@@ -525,6 +525,13 @@ class Batch:
         """The precision (abi.FP64 / abi.MIXED) each realisation runs in."""
         return self.work()[0]
 
+    def error_estimates(self):
+        """Per realisation: orders x the FP32 rounding residuals mixed
+        precision leaves uncorrected (ss_batch_error_estimates)."""
+        out = np.zeros(max(self.count, 1))
+        check(self.lib.ss_batch_error_estimates(self.handle, _d(out)))
+        return out[: self.count]
+
     def work(self):
         """(precision, amplitude-orders per run) of each realisation."""
         prec = np.zeros(max(self.count, 1), dtype=np.int32)

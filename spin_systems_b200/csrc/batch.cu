@@ -1060,6 +1060,7 @@ struct ss_batch {
   int64_t launches_per_run = 0;
   std::vector<int32_t> real_precision;  // ss_precision per realisation, index order
   std::vector<double> real_amp_orders;  // amplitudes x orders per realisation
+  std::vector<double> real_error_estimate;  // mixed precision: orders x uncorrected residual
   // device
   Op* d_ops = nullptr;
   double* d_rots = nullptr;
@@ -1184,8 +1185,44 @@ void coefficient_block(int L, const double* f, const std::vector<PairTerm>& pair
   }
 }
 
+// Sum of the FP32 rounding residuals a mixed-precision table leaves
+// uncorrected: every coupling channel except the kCorr strongest (whose
+// residuals coefficient_block hands to the kernel) and the transverse
+// fields, all in the table's scaled units.  The kernel applies this
+// perturbation of H at every order, coherently, so orders x residual sum
+// estimates the echo error a realisation accumulates in mixed precision.
+double uncorrected_residual(int L, const double* f, const std::vector<PairTerm>& pairs,
+                            double scale) {
+  const size_t P = pairs.size();
+  std::vector<double> ff(P), fb(P);
+  auto rounding = [](double c) { return std::abs(c - static_cast<double>(static_cast<float>(c))); };
+  for (size_t p = 0; p < P; ++p) {
+    const double q = scale * 0.25;
+    const double a = q * (pairs[p].jx + pairs[p].jy), b = q * (pairs[p].jx - pairs[p].jy);
+    ff[p] = std::abs(a) > kNegligible ? a : 0.0;
+    fb[p] = std::abs(b) > kNegligible ? b : 0.0;
+  }
+  std::vector<size_t> idx(P);
+  std::iota(idx.begin(), idx.end(), size_t{0});
+  std::stable_sort(idx.begin(), idx.end(), [&](size_t x, size_t y) {
+    return std::abs(ff[x]) + std::abs(fb[x]) > std::abs(ff[y]) + std::abs(fb[y]);
+  });
+  double sum = 0.0;
+  for (size_t r = static_cast<size_t>(kCorr); r < P; ++r) {
+    sum += rounding(ff[idx[r]]) + rounding(fb[idx[r]]);
+  }
+  for (int s = 0; s < L; ++s) {
+    const double cx = scale * 0.5 * f[3 * s], cy = scale * 0.5 * f[3 * s + 1];
+    if (std::abs(cx) > kNegligible || std::abs(cy) > kNegligible) {
+      sum += rounding(cx) + rounding(cy);
+    }
+  }
+  return sum;
+}
+
 struct PerReal {
   int L = 0;
+  double error_estimate = 0.0;  // orders x uncorrected residual, both vectors
   double tau_draw = 1.0;
   std::vector<int2> pairs;
   std::vector<double> psi0;
@@ -1275,9 +1312,20 @@ void build_realization(const ss_run_config& c, uint64_t index, const std::vector
       orders[t] = static_cast<int>(exps.back().order());
     }
     int64_t per_state = 0;
-    for (const Op& op : ops) {
-      if (op.kind == OP_EVOLVE) per_state += static_cast<int64_t>(orders[op.a]) * op.b;
+    std::vector<double> residual(keys.size(), 0.0);
+    for (size_t t = 0; t < keys.size(); ++t) {
+      if (orders[t] > 0) {
+        residual[t] = uncorrected_residual(L, tables[t], rz.pairs, -2.0 / exps[t].bound);
+      }
     }
+    double estimate = 0.0;
+    for (const Op& op : ops) {
+      if (op.kind == OP_EVOLVE) {
+        per_state += static_cast<int64_t>(orders[op.a]) * op.b;
+        estimate += 2.0 * static_cast<double>(orders[op.a]) * op.b * residual[op.a];
+      }
+    }
+    out.error_estimate = estimate;
     out.mixed = mixed && stays_mixed(c, L, per_state);
     for (size_t t = 0; t < keys.size(); ++t) {
       const TypeKey& k = keys[t];
@@ -1436,6 +1484,7 @@ void build_plan(ss_batch* b, const ss_run_config& c) {
     by_size[{pr.L, pr.mixed}].push_back(static_cast<int>(i));
     b->real_precision.push_back(pr.mixed ? SS_PRECISION_MIXED : SS_PRECISION_FP64);
     b->real_amp_orders.push_back(pr.amp_orders);
+    b->real_error_estimate.push_back(pr.error_estimate);
   }
   b->state_len = state_off;
   b->rows_len = row_off;
@@ -1833,6 +1882,13 @@ int ss_batch_io_bytes(const ss_batch* b, int64_t* h2d, int64_t* d2h) {
     for (const Bucket& bk : b->buckets) in += static_cast<int64_t>(sizeof(int) * bk.work.size());
     if (h2d) *h2d = in;
     if (d2h) *d2h = static_cast<int64_t>(sizeof(double) * b->rows_len + sizeof(int));
+  });
+}
+
+int ss_batch_error_estimates(const ss_batch* b, double* estimate) {
+  return guarded([&] {
+    require(b != nullptr && estimate != nullptr, SS_ERR_INVALID_ARGUMENT, "null argument");
+    std::copy(b->real_error_estimate.begin(), b->real_error_estimate.end(), estimate);
   });
 }
 

@@ -87,13 +87,20 @@ def uneven(args) -> dict:
            "tuning_seconds": tune_s}
     # The FP64 reference: the plain path on a sample of each size, which also
     # gives the echo error of those curves.
+    # The sample of each size is spread over its work distribution: the
+    # size's realisations sorted by amplitude-orders, one taken at evenly
+    # spaced ranks (lightest to heaviest).
     errs = {}
     plain = {}
     samples = {}
-    plain_total = 0.0
+    spread = {}
+    per_size_rate = {}  # seconds per amplitude-order of each sampled curve
+    run_realization(eng, cfg, 0, b.points, b.width)  # warm-up
     for L in np.unique(sizes):
         members = np.flatnonzero(sizes == L)
-        idx = members[: args.plain_sample]
+        order = members[np.argsort(amp[members], kind="stable")]
+        k = min(args.plain_sample, len(order))
+        idx = order[np.unique(np.round(np.linspace(0, len(order) - 1, k)).astype(int))]
         ts, es = [], []
         scale = corr0(cfg, idx, 16)
         for j, i in enumerate(idx):
@@ -101,20 +108,77 @@ def uneven(args) -> dict:
             _, ref = run_realization(eng, cfg, int(i), b.points, b.width)
             ts.append(time.perf_counter() - t0)
             es.append(float(np.abs(mixed[i, :, 0] - ref[:, 0]).max() / scale[j]))
-        # seconds per amplitude-order of the sample, times the size's work
-        size_s = sum(ts) * float(amp[members].sum()) / float(amp[idx].sum())
-        plain_total += size_s
-        plain[int(L)] = size_s / len(members)
-        samples[int(L)] = len(idx)
+        rate = np.array(ts) / amp[idx]
+        per_size_rate[int(L)] = (members, rate)
+        plain[int(L)] = float(rate.mean() * amp[members].mean())
+        samples[int(L)] = int(len(idx))
+        spread[int(L)] = {"ns_per_amp_order_min": float(rate.min() * 1e9),
+                          "ns_per_amp_order_max": float(rate.max() * 1e9),
+                          "ns_per_amp_order_cv": float(rate.std() / rate.mean())}
         errs[int(L)] = {"max": max(es), "mean": float(np.mean(es))}
+    # The batch's plain time: each size's amplitude-orders times its sampled
+    # mean seconds per amplitude-order; a bootstrap over the samples gives the
+    # spread of the ratio.
+    def plain_total_for(pick):
+        return sum(float(amp[m].sum()) * float(r[pick(r)].mean()) for m, r in per_size_rate.values())
+    plain_total = plain_total_for(lambda r: np.arange(len(r)))
+    rng = np.random.default_rng(20240726)
+    boots = [plain_total_for(lambda r: rng.integers(0, len(r), len(r))) for _ in range(2000)]
+    ratio = (n / dev_s) / (n / plain_total)
+    lo, hi = np.percentile([(n / dev_s) / (n / t) for t in boots], [2.5, 97.5])
     rep["plain_fp64"] = {"seconds_per_realization": plain, "sampled": samples,
-                         "curves_per_s": n / plain_total,
-                         "note": "one realisation at a time through ss_run_realization, "
-                                 "timed on the sampled realisations of each size and scaled "
-                                 "by that size's amplitude-orders in the batch"}
-    rep["speedup_batched_mixed_over_plain_fp64"] = (n / dev_s) / (n / plain_total)
+                         "spread": spread, "curves_per_s": n / plain_total,
+                         "note": "one realisation at a time through ss_run_realization on a "
+                                 "sample of each size spread over its amplitude-orders; the "
+                                 "size's time is its amplitude-orders times the sample's mean "
+                                 "seconds per amplitude-order"}
+    rep["speedup_batched_mixed_over_plain_fp64"] = ratio
+    rep["speedup_95pct_bootstrap"] = [float(lo), float(hi)]
     rep["echo_error_vs_plain_fp64"] = errs
     b._destroy()
+    eng.close()
+    return rep
+
+
+def routing(args) -> dict:
+    """Mixed precision with no FP64 routing against batched FP64 on the same
+    realisations: per curve, the echo error (max over time of |corr_x
+    mixed - FP64| / <ref|ref>), the batch's error estimate (orders x the FP32
+    rounding residuals the kernel leaves uncorrected) and the orders per
+    state vector (the order-count rule's input)."""
+    eng = Engine(0)
+    rep = {}
+    for L, n in zip(args.sizes, args.counts):
+        if args.program == "xy8":
+            spec = workloads.xy8_finite(nspins=L, realizations=n)
+        else:
+            spec = workloads.cpmg_uneven(realizations=n)
+            spec.spin_choices = (L,)
+        spec.mixed_order_limit = -1
+        cfg = spec.config()
+        bm = Batch(eng, cfg, 0, n, abi.MIXED)
+        _, mixed = bm.run()
+        est = bm.error_estimates()
+        _, amp = bm.work()
+        bm._destroy()
+        b64 = Batch(eng, cfg, 0, n, abi.FP64)
+        _, fp64 = b64.run()
+        b64._destroy()
+        scale = corr0(cfg, range(n), 16)
+        err = np.abs(mixed[:, :, 0] - fp64[:, :, 0]).max(axis=1) / scale
+        orders = amp / float(2 << L)
+        rep[int(L)] = {"program": args.program, "realizations": n,
+                       "echo_error": [float(x) for x in err],
+                       "estimate": [float(x) for x in est],
+                       "orders_per_state": [float(x) for x in orders],
+                       "amplitude_orders": [float(x) for x in amp],
+                       "max_error": float(err.max())}
+        print(json.dumps({int(L): {"max_error": float(err.max()),
+                                   "corr_log_est": float(np.corrcoef(np.log(err + 1e-300),
+                                                                     np.log(est + 1e-300))[0, 1]),
+                                   "corr_log_orders": float(np.corrcoef(np.log(err + 1e-300),
+                                                                        np.log(orders))[0, 1])}}),
+              flush=True)
     eng.close()
     return rep
 
@@ -327,7 +391,7 @@ def main(argv=None) -> None:
     u.add_argument("--warmup", type=int, default=0,
                    help="untimed runs first (the graph is instantiated at creation)")
     u.add_argument("--tune-sample", type=int, default=64)
-    u.add_argument("--plain-sample", type=int, default=2)
+    u.add_argument("--plain-sample", type=int, default=8)
     u.add_argument("--out", default="")
     lo = sub.add_parser("long")
     lo.add_argument("--nspins", type=int, default=16)
@@ -346,6 +410,11 @@ def main(argv=None) -> None:
     pl.add_argument("--gather-max", type=int, default=30,
                     help="largest L timed with the gather kernel")
     pl.add_argument("--out", default="")
+    ro = sub.add_parser("routing")
+    ro.add_argument("--program", choices=["xy8", "cpmg"], default="xy8")
+    ro.add_argument("--sizes", type=int, nargs="+", default=[12, 14, 16])
+    ro.add_argument("--counts", type=int, nargs="+", default=[1024, 296, 72])
+    ro.add_argument("--out", default="")
     ps = sub.add_parser("per_size")
     ps.add_argument("--sizes", type=int, nargs="+", default=[12, 14, 16])
     ps.add_argument("--counts", type=int, nargs="+", default=[1184, 592, 112])
@@ -353,7 +422,7 @@ def main(argv=None) -> None:
     ps.add_argument("--out", default="")
     args = ap.parse_args(argv)
     rep = {"uneven": uneven, "long": long_run, "plain": plain,
-           "per_size": per_size}[args.cmd](args)
+           "per_size": per_size, "routing": routing}[args.cmd](args)
     text = json.dumps(rep, indent=1)
     print(text)
     if args.out:
