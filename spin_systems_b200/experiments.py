@@ -155,6 +155,8 @@ def routing(args) -> dict:
             spec = workloads.cpmg_uneven(realizations=n)
             spec.spin_choices = (L,)
         spec.mixed_order_limit = -1
+        if args.norm:
+            spec.observables = ["corr:x", "norm"]
         cfg = spec.config()
         bm = Batch(eng, cfg, 0, n, abi.MIXED)
         _, mixed = bm.run()
@@ -167,7 +169,17 @@ def routing(args) -> dict:
         scale = corr0(cfg, range(n), 16)
         err = np.abs(mixed[:, :, 0] - fp64[:, :, 0]).max(axis=1) / scale
         orders = amp / float(2 << L)
+        if args.norm:
+            # columns: corr re, corr im, |psi|, |ref|; drift against FP64
+            drift = np.maximum(np.abs(mixed[:, :, 2] - fp64[:, :, 2]).max(axis=1),
+                               np.abs(mixed[:, :, 3] - fp64[:, :, 3]).max(axis=1)
+                               / np.sqrt(scale))
+            # against the exact initial norms: |psi0| = 1, |ref0| = sqrt(<ref|ref>)
+            self_drift = np.maximum(np.abs(mixed[:, :, 2] - 1.0).max(axis=1),
+                                    np.abs(mixed[:, :, 3] - np.sqrt(scale)[:, None]).max(axis=1)
+                                    / np.sqrt(scale))
         rep[int(L)] = {"program": args.program, "realizations": n,
+                       "norm_drift": [float(x) for x in self_drift] if args.norm else None,
                        "echo_error": [float(x) for x in err],
                        "estimate": [float(x) for x in est],
                        "orders_per_state": [float(x) for x in orders],
@@ -414,6 +426,8 @@ def main(argv=None) -> None:
     ro.add_argument("--program", choices=["xy8", "cpmg"], default="xy8")
     ro.add_argument("--sizes", type=int, nargs="+", default=[12, 14, 16])
     ro.add_argument("--counts", type=int, nargs="+", default=[1024, 296, 72])
+    ro.add_argument("--norm", action="store_true",
+                    help="also measure the state and reference norms (drift per curve)")
     ro.add_argument("--out", default="")
     ps = sub.add_parser("per_size")
     ps.add_argument("--sizes", type=int, nargs="+", default=[12, 14, 16])
