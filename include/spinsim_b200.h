@@ -146,10 +146,10 @@ typedef struct ss_run_config {
   int32_t spin_choices[8];
   /* additive: in SS_PRECISION_MIXED, a realisation whose Chebyshev orders
      per state vector exceed this runs in the FP64 kernel of the same batch
-     (FP32 coefficient rounding grows with the order count); 0 = 40000
-     for L <= 15 with L = 16 staying mixed (its FP64 kernel takes the heavy
-     tail one 16-CTA cluster each), > 0 = that limit at every size,
-     negative = never. */
+     (the FP32 recursion's rounding error grows with the order count and
+     shrinks with L); 0 = the measured per-size limits (7400 orders at
+     L = 8, 11600 at 10, 38600 at 12, 97000 at 14, L = 16 staying mixed),
+     > 0 = that limit at every size, negative = never. */
   int64_t mixed_order_limit;
   /* additive: a parameter sweep for the batched engine.  With
      sweep_points = P > 0 a batch of `count` realisations is P consecutive

@@ -1269,22 +1269,28 @@ void exact_transverse(int L, const double* f, int mode, double tau, Expansion& e
   ex.bound = bound2;
 }
 
-constexpr int64_t kDefaultMixedOrderLimit = 40000;
-// Largest size the default limit routes.  L = 16's FP64 kernel (16-CTA split
-// clusters) takes its heaviest realisations one cluster each: on B200 routing
-// them halves the size's batch rate, while mixed runs stay within 3e-7 of
-// FP64 in the correlation over ~5e5 orders per state at L = 16.
-constexpr int kDefaultRouteMaxL = 15;
+// Default routing of mixed batches: a realisation whose Chebyshev orders per
+// state vector exceed its size's limit runs in FP64.  Measured on B200 with
+// routing off (1024-2048 realisations per size of the CPMG and XY-8
+// programs): the echo error of a mixed curve grows as orders^0.86 and falls
+// with L (the FP32 rounding of 2^L amplitudes averages out in the overlap),
+// so the order count at which the first curve passes 1e-6 grows by ~1.5x
+// per spin: 9.3K / 14.5K / 48K / 121K orders at L = 8 / 10 / 12 / 14, none at
+// L = 16 (max 2.7e-7 at 1.1e5 orders).  The limits are those counts times
+// 0.8 (interpolated for odd L); L = 16 is not routed by default.
+// `mixed_order_limit` > 0 replaces them by one limit for every size; < 0
+// keeps every realisation mixed.
+constexpr int64_t kDefaultMixedOrderLimit[17] = {
+    2000, 2000, 2000, 2000, 2000, 2000,  // L < 6 has no batched kernel
+    3500, 5000, 7400, 9500, 11600, 21000, 38600, 60000, 97000, 150000,
+    std::numeric_limits<int64_t>::max()};
 
-// Mixed precision stores every coefficient as one FP32 number; the rounding
-// is a fixed perturbation of the Hamiltonian whose effect on the echo grows
-// with the number of orders applied.  A realisation past `limit` orders per
-// state vector therefore runs in FP64 (when its size has an FP64 kernel; with
-// the default limit, up to kDefaultRouteMaxL).
 bool stays_mixed(const ss_run_config& c, int L, int64_t orders_per_state) {
-  const int64_t limit = c.mixed_order_limit == 0 ? kDefaultMixedOrderLimit : c.mixed_order_limit;
-  if (limit < 0 || orders_per_state <= limit) return true;
-  if (c.mixed_order_limit == 0 && L > kDefaultRouteMaxL) return true;
+  if (c.mixed_order_limit < 0) return true;
+  const int64_t limit = c.mixed_order_limit > 0
+                            ? c.mixed_order_limit
+                            : kDefaultMixedOrderLimit[std::min(std::max(L, 0), 16)];
+  if (orders_per_state <= limit) return true;
   return find_variant(L, false) == nullptr;
 }
 

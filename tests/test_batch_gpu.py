@@ -118,14 +118,15 @@ def orders_per_state(port, spec, count):
 
 
 def test_mixed_routes_long_realisations_to_fp64(engine, port):
-    # Full XY-8 x 16 at L = 12: realisations past 40000 orders per state run
-    # in the FP64 kernel of the same batch, bit-identical to an FP64 batch.
+    # Full XY-8 x 16 at L = 12: realisations past the size's default limit
+    # (38600 orders per state) run in the FP64 kernel of the same batch,
+    # bit-identical to an FP64 batch.
     n = 192
     spec = workloads.xy8_finite(realizations=n)
     orders = orders_per_state(port, spec, n)
     b = ss.Batch(engine, spec.config(), 0, n, abi.MIXED)
     prec = b.precisions()
-    assert np.array_equal(prec == abi.FP64, orders > 40000)
+    assert np.array_equal(prec == abi.FP64, orders > 38600)
     assert (prec == abi.FP64).any() and (prec == abi.MIXED).any()
     _, mixed = b.run()
     _, fp64 = run(engine, spec, n, abi.FP64)
