@@ -341,8 +341,16 @@ def run_ours(args):
     fma_peak = 2.0 * 128.0 * eng_sms() * mhz * 1e6 / 1e12
     fma_ach = FLOPS_PER_AMP_ORDER * amp_mixed / (ms_step / 1e3) / 1e12
     threads = cpu_threads()
-    cb = reference_sample(spec, 2 * threads, threads, CPU_SAMPLE_SEED + 2)
-    cb1 = reference_sample(spec, 1, 1, CPU_SAMPLE_SEED + 3)
+    cb = reference_sample(spec, 3 * threads, threads, CPU_SAMPLE_SEED + 2)
+    cb1 = reference_sample(spec, 2, 1, CPU_SAMPLE_SEED + 3)
+    # Realisations differ ~10x in work: the CPU's seconds per amplitude-order
+    # on its sample, times the batch's amplitude-orders, is the rate the
+    # whole batch would run at.
+    amp_all = np.asarray(amp_each, dtype=np.float64)
+    for c, seed, count in ((cb, CPU_SAMPLE_SEED + 2, 3 * threads), (cb1, CPU_SAMPLE_SEED + 3, 2)):
+        pick = [int(i) for i in seeded_subset(count, REALIZATIONS, seed)]
+        c["amplitude_order_scaled"] = (len(amp_all) / (c["seconds"] / amp_all[pick].sum()
+                                                         * amp_all.sum()))
     sizes = per_size_ratios(eng, args) if args.per_size else {}
     kern = plain_order_kernels(eng, hbm) if args.plain_kernels else {}
     line = {
@@ -382,7 +390,8 @@ def run_ours(args):
         "plain_order_kernel_hbm": kern,
         "routing": {"fp64_realizations": int(routed.sum()), "realizations": int(len(prec)),
                     "fp64_amplitude_order_share": amp_fp64 / amp_orders,
-                    "rule": "more than 40000 Chebyshev orders per state vector -> FP64 kernel"},
+                    "rule": "more than the size's order limit per state vector (38600 at "
+                            "L = 12) -> FP64 kernel of the same graph"},
         "clocks": clk,
         "echo_error": {"max": float(err.max()), "mean": float(err.mean()), "curves": check,
                        "above_1e-6": int((err > 1e-6).sum()),
@@ -392,8 +401,9 @@ def run_ours(args):
         "per_size_cpmg32": sizes,
         "work": {"amplitude_orders_per_step": amp_orders, "orders_per_step": stats["orders"]},
         "cpu_baseline": dict({k: cb[k] for k in ("value", "unit", "cores", "kind", "sample",
-                                                 "model")},
-                             one_thread={k: cb1[k] for k in ("value", "unit", "sample")}),
+                                                 "model", "amplitude_order_scaled")},
+                             one_thread={k: cb1[k] for k in ("value", "unit", "sample",
+                                                             "amplitude_order_scaled")}),
         "schedule": ({"tuned": [{k: r[k] for k in ("L", "precision", "variant", "ns")} for r in tuned],
                       "tuning_seconds": tune_s, "sample": args.tune_sample}
                      if args.tune else {"tuned": [], "note": "default schedules (--no-tune)"}),

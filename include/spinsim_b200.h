@@ -148,7 +148,7 @@ typedef struct ss_run_config {
      per state vector exceed this runs in the FP64 kernel of the same batch
      (the FP32 recursion's rounding error grows with the order count and
      shrinks with L); 0 = the measured per-size limits (7400 orders at
-     L = 8, 11600 at 10, 38600 at 12, 97000 at 14, L = 16 staying mixed),
+     L = 8, 11600 at 10, 38600 at 12, 40000 at 13..15, L = 16 staying mixed),
      > 0 = that limit at every size, negative = never. */
   int64_t mixed_order_limit;
   /* additive: a parameter sweep for the batched engine.  With

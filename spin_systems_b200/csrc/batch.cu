@@ -1276,13 +1276,17 @@ void exact_transverse(int L, const double* f, int mode, double tau, Expansion& e
 // with L (the FP32 rounding of 2^L amplitudes averages out in the overlap),
 // so the order count at which the first curve passes 1e-6 grows by ~1.5x
 // per spin: 9.3K / 14.5K / 48K / 121K orders at L = 8 / 10 / 12 / 14, none at
-// L = 16 (max 2.7e-7 at 1.1e5 orders).  The limits are those counts times
-// 0.8 (interpolated for odd L); L = 16 is not routed by default.
-// `mixed_order_limit` > 0 replaces them by one limit for every size; < 0
-// keeps every realisation mixed.
+// L = 16 (max 2.7e-7 at 1.1e5 orders).  Up to L = 12 the limits are those
+// counts times 0.8 (interpolated for odd L).  At L = 13..15 they stay at
+// 40000, below what accuracy needs: the FP64 bucket's wider clusters finish
+// the heavy tail sooner than the mixed bucket's split clusters, so routing
+// it shortens the batch (L = 14 CPMG-32, 296 realisations: 39.0 curves/s at
+// 40000, 24.7 at 97000).  L = 16 is not routed by default (its FP64 kernel
+// needs 16-CTA clusters).  `mixed_order_limit` > 0 replaces the limits by one
+// for every size; < 0 keeps every realisation mixed.
 constexpr int64_t kDefaultMixedOrderLimit[17] = {
     2000, 2000, 2000, 2000, 2000, 2000,  // L < 6 has no batched kernel
-    3500, 5000, 7400, 9500, 11600, 21000, 38600, 60000, 97000, 150000,
+    3500, 5000, 7400, 9500, 11600, 21000, 38600, 40000, 40000, 40000,
     std::numeric_limits<int64_t>::max()};
 
 bool stays_mixed(const ss_run_config& c, int L, int64_t orders_per_state) {
