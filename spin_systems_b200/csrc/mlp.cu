@@ -5,13 +5,14 @@
 // Every matrix product -- the four forward layers, the backward data products
 // and the weight gradients -- is one kernel, k_gemm:
 //     C[M][N] = A[M][K] . B[N][K]^T,   A and B K-major BF16 in global memory.
-// One CTA of four warps owns a 128-row tile of C across its whole width
-// (N <= 256).  Warp 0 stages 64-wide K slices of A and B into shared memory
-// with TMA (128-byte swizzle) through a four-deep ring of mbarriers; warp 1
-// issues tcgen05.mma (kind::f16, BF16 x BF16 -> FP32, M = 128, N = width,
-// K = 16 per instruction) into a TMEM accumulator of N columns and hands each
-// stage back with tcgen05.commit; then all four warps read the accumulator
-// with tcgen05.ld (TMEM lane = row of the tile) through a fused epilogue:
+// One CTA of four warps owns a 128-row x BN-column tile of C (BN = 32..256,
+// picked per product so the grid covers the device).  Warp 0 stages 64-wide
+// K slices of A and B into shared memory with TMA (128-byte swizzle) through
+// a four-deep ring of mbarriers; warp 1 issues tcgen05.mma (kind::f16,
+// BF16 x BF16 -> FP32, M = 128, N = BN, K = 16 per instruction) into a TMEM
+// accumulator of BN columns and hands each stage back with tcgen05.commit;
+// then all four warps read the accumulator with tcgen05.ld (TMEM lane = row
+// of the tile) through a fused epilogue:
 //   EPI_HIDDEN  z = acc + b, stored FP32; h = GELU(z) stored BF16 and, for
 //               training, transposed (h^T is the K-major operand of the next
 //               layer's weight gradient);
@@ -19,6 +20,8 @@
 //   EPI_BACK    dz = acc * GELU'(z_below), stored FP32 (bias gradient),
 //               BF16 and transposed BF16;
 //   EPI_F32     plain FP32 store (weight gradients).
+// The transposed BF16 tile is staged in the (by then idle) operand ring as
+// [BN][128] and written back as 256-byte column runs with 16-byte stores.
 // Waits on mbarriers are bounded by the global timer: a wait that runs out
 // sets an error flag, the CTA still drains what it issued, frees its TMEM and
 // returns, and the host reports SS_ERR_TIMEOUT.
@@ -61,6 +64,7 @@ enum Epi { EPI_HIDDEN = 0, EPI_OUT = 1, EPI_BACK = 2, EPI_F32 = 3 };
 
 struct GemmArgs {
   int M, N, K;
+  int bn;                  // columns of C per CTA (gridDim.z = N / bn)
   const float* bias;       // HIDDEN, OUT: N
   float* out_f32;          // HIDDEN: z; OUT: y; BACK: dz; F32: C   ([M][N])
   __nv_bfloat16* out_bf;   // HIDDEN: GELU(z); BACK: dz             ([M][N])
@@ -71,9 +75,12 @@ struct GemmArgs {
   float* partial;          // splits > 1: [splits][M][N] FP32 slices, summed by k_splitk_sum
 };
 
-size_t gemm_smem(int N) {
-  return 1024 /* alignment slack */ + size_t{kStages} * (kABytes + size_t(N) * BK * 2) + 256;
+size_t gemm_smem(int bn) {
+  return 1024 /* alignment slack */ + size_t{kStages} * (kABytes + size_t(bn) * BK * 2) + 256;
 }
+// The staged transposed tile ([bn][BM] BF16) fits in the B part of the
+// operand ring it reuses ([kStages][bn][BK] BF16), whatever bn is.
+static_assert(BM <= kStages * BK, "transposed staging outgrows the operand ring");
 
 // ------------------------------------------------------------ PTX helpers
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -199,8 +206,10 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
   // 1024-byte alignment in the shared window: the 128-byte swizzle pattern
   // of TMA and of the MMA descriptors is anchored there.
   uint8_t* base = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
-  const int N = a.N;
-  const uint32_t b_bytes = uint32_t(N) * BK * 2;
+  const int N = a.N;    // full width of C (row stride of the outputs)
+  const int BN = a.bn;  // this CTA's columns: [n0, n0 + BN)
+  const int n0 = blockIdx.z * BN;
+  const uint32_t b_bytes = uint32_t(BN) * BK * 2;
   const uint32_t stage_bytes = kABytes + b_bytes;
   uint64_t* bars = reinterpret_cast<uint64_t*>(base + kStages * stage_bytes);
   uint64_t* full = bars;                  // TMA -> MMA
@@ -210,7 +219,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
   __shared__ int s_fail;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t ncols = N <= 32 ? 32u : (N <= 64 ? 64u : (N <= 128 ? 128u : 256u));
+  const uint32_t ncols = BN <= 32 ? 32u : (BN <= 64 ? 64u : (BN <= 128 ? 128u : 256u));
 
   if (threadIdx.x == 0) {
     s_fail = 0;
@@ -240,7 +249,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
 
   if (warp == 0) {
     if (lane == 0) {
-      // Producer: stage k-slices of A (128 rows) and B (N rows).
+      // Producer: stage k-slices of A (128 rows) and B (BN rows).
       int issued = 0;
       bool ok = true;
       for (int kt = 0; kt < nk && ok; ++kt) {
@@ -253,7 +262,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         const uint32_t fb = smem_u32(&full[s]);
         mbar_expect_tx(fb, stage_bytes);
         tma_load_2d(smem_u32(sa), &map_a, fb, (kbase + kt) * BK, m0);
-        tma_load_2d(smem_u32(sa + kABytes), &map_b, fb, (kbase + kt) * BK, 0);
+        tma_load_2d(smem_u32(sa + kABytes), &map_b, fb, (kbase + kt) * BK, n0);
         ++issued;
       }
       if (!ok) atomicExch(&s_fail, 1);
@@ -266,7 +275,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
   } else if (warp == 1) {
     if (lane == 0) {
       // MMA issuer.
-      const uint32_t idesc = idesc_bf16(BM, N);
+      const uint32_t idesc = idesc_bf16(BM, BN);
       for (int kt = 0; kt < nk; ++kt) {
         const int s = kt % kStages;
         if (!mbar_wait(smem_u32(&full[s]), (kt / kStages) & 1)) {
@@ -296,15 +305,19 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
   if (good) {
     const int row = m0 + warp * 32 + lane;
     const int M = a.M;
-    for (int c0 = 0; c0 < N; c0 += 16) {
+    // The operand ring is idle once `done` completed: every copy landed and
+    // every MMA that read it finished.  It holds the transposed BF16 tile.
+    __nv_bfloat16* stage_t = reinterpret_cast<__nv_bfloat16*>(base);
+    for (int c0 = 0; c0 < BN; c0 += 16) {
+      const int col = n0 + c0;
       float v[16];
       tmem_ld16(tmem + (uint32_t(warp * 32) << 16) + uint32_t(c0), v);
       if (EPI == EPI_HIDDEN || EPI == EPI_OUT) {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) v[j] += a.bias[c0 + j];
+        for (int j = 0; j < 16; ++j) v[j] += a.bias[col + j];
       }
       if (EPI == EPI_BACK) {
-        const float4* zp = reinterpret_cast<const float4*>(a.zin + size_t(row) * N + c0);
+        const float4* zp = reinterpret_cast<const float4*>(a.zin + size_t(row) * N + col);
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
           const float4 z = zp[q];
@@ -317,20 +330,32 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
       float* out = (EPI == EPI_F32 && a.splits > 1)
                        ? a.partial + size_t(blockIdx.y) * size_t(M) * N
                        : a.out_f32;
-      float4* fp = reinterpret_cast<float4*>(out + size_t(row) * N + c0);
+      float4* fp = reinterpret_cast<float4*>(out + size_t(row) * N + col);
 #pragma unroll
       for (int q = 0; q < 4; ++q) fp[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
       if (EPI == EPI_HIDDEN || EPI == EPI_BACK) {
         __nv_bfloat16 hb[16];
 #pragma unroll
         for (int j = 0; j < 16; ++j) hb[j] = __float2bfloat16_rn(EPI == EPI_HIDDEN ? gelu(v[j]) : v[j]);
-        uint4* bp = reinterpret_cast<uint4*>(a.out_bf + size_t(row) * N + c0);
+        uint4* bp = reinterpret_cast<uint4*>(a.out_bf + size_t(row) * N + col);
         bp[0] = *reinterpret_cast<const uint4*>(&hb[0]);
         bp[1] = *reinterpret_cast<const uint4*>(&hb[8]);
         if (a.out_bt) {
+          // A warp's 32 rows of one column are 64 contiguous bytes here.
 #pragma unroll
-          for (int j = 0; j < 16; ++j) a.out_bt[size_t(c0 + j) * M + row] = hb[j];
+          for (int j = 0; j < 16; ++j) stage_t[(c0 + j) * BM + warp * 32 + lane] = hb[j];
         }
+      }
+    }
+    if ((EPI == EPI_HIDDEN || EPI == EPI_BACK) && a.out_bt) {
+      __syncthreads();
+      // Column c of the tile is rows m0 .. m0 + 127 of row n0 + c of C^T:
+      // 16 stores of 16 bytes, consecutive threads on consecutive addresses.
+      const uint4* src = reinterpret_cast<const uint4*>(stage_t);
+      constexpr int kPerCol = BM / 8;
+      for (int i = threadIdx.x; i < BN * kPerCol; i += kGemmThreads) {
+        const int c = i / kPerCol, r8 = i % kPerCol;
+        *reinterpret_cast<uint4*>(a.out_bt + size_t(n0 + c) * M + m0 + r8 * 8) = src[i];
       }
     }
   } else if (threadIdx.x == 0) {
@@ -360,63 +385,127 @@ __global__ void k_splitk_sum(const float4* __restrict__ part, int splits, size_t
 }
 
 // ------------------------------------------------------- small kernels
+// Rows per block of the batch kernels below: 256 threads, one warp per four
+// rows for the 128-wide rows, one thread per 8-row x 1-column piece of a
+// transposed row block.
+constexpr int kRowBlock = 32;
+constexpr int kRowThreads = 256;
+constexpr int kTPitch = kRowBlock + 2;  // staged transposes: [column][row], padded
+
 // Builds one batch: rows of the data set named by idx (or zero rows where
 // idx < 0) as the padded BF16 input, its transpose, and the FP32 targets.
 // With `cursor` (training graphs) the batch is rows cursor[0] * rows .. of idx.
-__global__ void k_gather(const float* __restrict__ data_x, const float* __restrict__ data_y,
-                         const int* __restrict__ idx_base, int rows, __nv_bfloat16* x,
-                         __nv_bfloat16* xt, float* target, const int* cursor) {
+// Every store is a whole 16-byte piece of a row (x, target) or of a
+// transposed row (xt, through shared memory).
+__global__ void __launch_bounds__(kRowThreads)
+    k_gather(const float* __restrict__ data_x, const float* __restrict__ data_y,
+             const int* __restrict__ idx_base, int rows, __nv_bfloat16* x, __nv_bfloat16* xt,
+             float* target, const int* cursor) {
+  __shared__ int s_row[kRowBlock];
+  __shared__ __nv_bfloat16 s_in[kIn][kRowBlock];
   const int* idx = cursor ? idx_base + size_t(cursor[0]) * rows : idx_base;
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r < rows) {
-    const int i = idx[r];
-#pragma unroll 1
-    for (int c = 0; c < kInPad; ++c) {
-      const float f = (i >= 0 && c < kIn) ? data_x[size_t(i) * kIn + c] : 0.0f;
-      const __nv_bfloat16 b = __float2bfloat16_rn(f);
-      x[size_t(r) * kInPad + c] = b;
-      xt[size_t(c) * rows + r] = b;
+  const int r0 = blockIdx.x * kRowBlock;
+  const int t = threadIdx.x;
+  if (t < kRowBlock) {
+    const int i = idx[r0 + t];
+    s_row[t] = i;
+#pragma unroll
+    for (int c = 0; c < kIn; ++c) {
+      s_in[c][t] = __float2bfloat16_rn(i >= 0 ? data_x[size_t(i) * kIn + c] : 0.0f);
     }
   }
+  __syncthreads();
+  {
+    // x: row t / 8, columns 8 (t % 8) .. + 7 (only the first piece is nonzero)
+    const int r = t >> 3, q = t & 7;
+    __align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int c = 8 * q + j;
+      v[j] = c < kIn ? s_in[c][r] : __float2bfloat16_rn(0.0f);
+    }
+    *reinterpret_cast<uint4*>(x + size_t(r0 + r) * kInPad + 8 * q) = *reinterpret_cast<const uint4*>(v);
+  }
+  {
+    // xt: column t / 4, rows 8 (t % 4) .. + 7 of the block
+    const int c = t >> 2, part = t & 3;
+    __align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) v[j] = c < kIn ? s_in[c][8 * part + j] : __float2bfloat16_rn(0.0f);
+    *reinterpret_cast<uint4*>(xt + size_t(c) * rows + r0 + 8 * part) = *reinterpret_cast<const uint4*>(v);
+  }
   if (target) {
-    // targets: one row per iteration, the block's threads over columns
-    for (int rr = blockIdx.x * blockDim.x; rr < min(rows, (blockIdx.x + 1) * blockDim.x); ++rr) {
-      const int i = idx[rr];
-      for (int c = threadIdx.x; c < kOut; c += blockDim.x) {
-        target[size_t(rr) * kOut + c] = i >= 0 ? data_y[size_t(i) * kOut + c] : 0.0f;
-      }
+    // targets: warp w copies rows 4w .. 4w + 3, 16 bytes per lane per row
+    const int w = t >> 5, lane = t & 31;
+    float4 v[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int i = s_row[4 * w + k];
+      v[k] = i >= 0 ? reinterpret_cast<const float4*>(data_y + size_t(i) * kOut)[lane]
+                    : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      reinterpret_cast<float4*>(target + size_t(r0 + 4 * w + k) * kOut)[lane] = v[k];
     }
   }
 }
 
 // Mean-squared error over the first `valid` rows and the gradient of the
 // output layer: g = 2 (y - t) / (valid * kOut), FP32, BF16 and transposed.
-__global__ void k_loss(const float* __restrict__ y, const float* __restrict__ t, int rows,
-                       int valid, float* g, __nv_bfloat16* dz, __nv_bfloat16* dzt,
-                       double* partial) {
-  __shared__ double red[kGemmThreads / 32];
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  double acc = 0.0;
+// Warp w of a block handles rows 4w .. 4w + 3 of its 32, lane l columns
+// 4l .. 4l + 3 (16-byte loads and stores along the rows); the transposed
+// BF16 block is staged in shared memory and written as 16-byte pieces.
+// The block's squared error is summed in a fixed order (deterministic).
+__global__ void __launch_bounds__(kRowThreads)
+    k_loss(const float* __restrict__ y, const float* __restrict__ t, int rows, int valid, float* g,
+           __nv_bfloat16* dz, __nv_bfloat16* dzt, double* partial) {
+  __shared__ __nv_bfloat16 s_t[kOut][kTPitch];
+  __shared__ double red[kRowThreads / 32];
+  const int r0 = blockIdx.x * kRowBlock;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const float scale = 2.0f / (float(valid) * float(kOut));
-  if (r < rows) {
-    for (int c = 0; c < kOut; ++c) {
-      const float d = r < valid ? y[size_t(r) * kOut + c] - t[size_t(r) * kOut + c] : 0.0f;
-      acc += double(d) * double(d);
-      const float gv = d * scale;
-      g[size_t(r) * kOut + c] = gv;
-      const __nv_bfloat16 b = __float2bfloat16_rn(gv);
-      dz[size_t(r) * kOut + c] = b;
-      dzt[size_t(c) * rows + r] = b;
+  double acc = 0.0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int rl = 4 * w + k, r = r0 + rl;
+    float d[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    if (r < valid) {
+      const float4 a = reinterpret_cast<const float4*>(y + size_t(r) * kOut)[lane];
+      const float4 b = reinterpret_cast<const float4*>(t + size_t(r) * kOut)[lane];
+      d[0] = a.x - b.x;
+      d[1] = a.y - b.y;
+      d[2] = a.z - b.z;
+      d[3] = a.w - b.w;
     }
+    __align__(8) __nv_bfloat16 hb[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      acc += double(d[j]) * double(d[j]);
+      d[j] *= scale;
+      hb[j] = __float2bfloat16_rn(d[j]);
+      s_t[4 * lane + j][rl] = hb[j];
+    }
+    reinterpret_cast<float4*>(g + size_t(r) * kOut)[lane] = make_float4(d[0], d[1], d[2], d[3]);
+    *reinterpret_cast<uint2*>(dz + size_t(r) * kOut + 4 * lane) = *reinterpret_cast<const uint2*>(hb);
   }
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  if (lane == 0) red[w] = acc;
   __syncthreads();
+  // dzt: column c, rows 8 part .. + 7 of the block; two pieces per thread
+#pragma unroll
+  for (int i = threadIdx.x; i < kOut * 4; i += kRowThreads) {
+    const int c = i >> 2, part = i & 3;
+    __align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) v[j] = s_t[c][8 * part + j];
+    *reinterpret_cast<uint4*>(dzt + size_t(c) * rows + r0 + 8 * part) = *reinterpret_cast<const uint4*>(v);
+  }
   if (threadIdx.x == 0) {
-    double s = 0.0;
-    for (int w = 0; w < int(blockDim.x >> 5); ++w) s += red[w];
-    partial[blockIdx.x] = s;
+    double sum = 0.0;
+    for (int k = 0; k < kRowThreads / 32; ++k) sum += red[k];
+    partial[blockIdx.x] = sum;
   }
 }
 
@@ -639,8 +728,8 @@ void dalloc(T** p, size_t n) {
 
 void launch_gemm(ss_engine* e, const Gemm& gm) {
   const GemmArgs& a = gm.args;
-  const dim3 grid(a.M / BM, a.splits);
-  const size_t smem = gemm_smem(a.N);
+  const dim3 grid(a.M / BM, a.splits, a.N / a.bn);
+  const size_t smem = gemm_smem(a.bn);
   switch (gm.epi) {
     case EPI_HIDDEN: launch(e, k_gemm<EPI_HIDDEN>, grid, kGemmThreads, smem, gm.ma, gm.mb, a); break;
     case EPI_OUT: launch(e, k_gemm<EPI_OUT>, grid, kGemmThreads, smem, gm.ma, gm.mb, a); break;
@@ -668,18 +757,35 @@ int splitk_for(int M, int K) {
   return s;
 }
 
+// Columns of C per CTA: halved from the full width (down to 32, and only
+// while it stays a multiple of 16 dividing the width) while the
+// grid of row tiles x K slices x column tiles has fewer CTAs than the device
+// has SMs.  Short-K products are bound by their epilogues, which then run on
+// more SMs with fewer columns each.
+int column_tile(int M, int N, int splits) {
+  int sms = 148;
+  int dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) {
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  }
+  int bn = N;
+  while (bn > 32 && bn % 32 == 0 && (M / BM) * splits * (N / bn) < sms) bn /= 2;
+  return bn;
+}
+
 Gemm make_gemm(int epi, const __nv_bfloat16* A, const __nv_bfloat16* B, int M, int N, int K,
-               int* flags) {
+               int* flags, int splits = 1) {
   require(M % BM == 0 && K % BK == 0 && N % 16 == 0 && N >= 16 && N <= 256, SS_ERR_RUNTIME,
           "GEMM shape outside the tcgen05 tiling");
   Gemm g{};
-  g.ma = make_map(A, M, K, BM);
-  g.mb = make_map(B, N, K, N);
   g.args.M = M;
   g.args.N = N;
   g.args.K = K;
   g.args.flags = flags;
-  g.args.splits = 1;
+  g.args.splits = splits;
+  g.args.bn = column_tile(M, N, splits);
+  g.ma = make_map(A, M, K, BM);
+  g.mb = make_map(B, N, K, g.args.bn);
   g.epi = epi;
   return g;
 }
@@ -733,7 +839,7 @@ void build(ss_mlp* n) {
     dalloc(&n->dz[i], size_t(B) * kHidden);
     dalloc(&n->dzt[i], size_t(B) * kHidden);
   }
-  dalloc(&n->loss_part, size_t(B / kGemmThreads));
+  dalloc(&n->loss_part, size_t(B / kRowBlock));
   dalloc(&n->col_part, size_t(B / kColRows + 1) * kHidden);
   n->idx_cap = B;
   dalloc(&n->idx, size_t(B));
@@ -757,9 +863,9 @@ void build(ss_mlp* n) {
   for (int l = kLayers - 1; l >= 0; --l) {
     const int slot = (3 - l) & 1;
     const __nv_bfloat16* inT = l == 0 ? n->xt : n->ht[l - 1];  // [in][B]
-    Gemm gw = make_gemm(EPI_F32, n->dzt[slot], inT, kRowsOut[l], kRowsIn[l], B, flags);
+    Gemm gw = make_gemm(EPI_F32, n->dzt[slot], inT, kRowsOut[l], kRowsIn[l], B, flags,
+                        splitk_for(kRowsOut[l], B));
     gw.args.out_f32 = n->gw[l];
-    gw.args.splits = splitk_for(kRowsOut[l], B);
     n->bwd_w[l] = gw;
     if (l >= 1) {
       Gemm gx = make_gemm(EPI_BACK, n->dz[slot], n->wt[l], B, kRowsIn[l], kRowsOut[l], flags);
@@ -809,8 +915,8 @@ void colsum(ss_mlp* n, int N, float* out) {
 void backward(ss_mlp* n, int valid, double* loss, int slot, const int* cursor = nullptr) {
   ss_engine* e = n->engine;
   const int B = n->batch;
-  const int nb = B / kGemmThreads;
-  launch(e, k_loss, dim3(nb), kGemmThreads, 0, n->y, n->target, B, valid, n->g, n->dz[0],
+  const int nb = B / kRowBlock;
+  launch(e, k_loss, dim3(nb), kRowThreads, 0, n->y, n->target, B, valid, n->g, n->dz[0],
          n->dzt[0], n->loss_part);
   launch(e, k_loss_total, dim3(1), 32, 0, n->loss_part, nb, valid, loss, slot, cursor);
   colsum(n, kOut, n->gb[3]);
@@ -826,7 +932,7 @@ void backward(ss_mlp* n, int valid, double* loss, int slot, const int* cursor = 
 void gather(ss_mlp* n, const float* dx, const float* dy, const int* idx,
             const int* cursor = nullptr) {
   const int B = n->batch;
-  launch(n->engine, k_gather, dim3(B / kGemmThreads), kGemmThreads, 0, dx, dy, idx, B, n->x,
+  launch(n->engine, k_gather, dim3(B / kRowBlock), kRowThreads, 0, dx, dy, idx, B, n->x,
          n->xt, dy ? n->target : nullptr, cursor);
 }
 
@@ -1163,9 +1269,8 @@ int ss_mlp_gemm_test(ss_engine* e, const uint16_t* a, const uint16_t* b, int M, 
       SS_CUDA(cudaMalloc(&dc, sizeof(float) * size_t(M) * N));
       SS_CUDA(cudaMemcpyAsync(da, a, sizeof(uint16_t) * size_t(M) * K, cudaMemcpyHostToDevice, e->stream));
       SS_CUDA(cudaMemcpyAsync(db, b, sizeof(uint16_t) * size_t(N) * K, cudaMemcpyHostToDevice, e->stream));
-      Gemm g = make_gemm(EPI_F32, da, db, M, N, K, e->dev_flags + 8);
+      Gemm g = make_gemm(EPI_F32, da, db, M, N, K, e->dev_flags + 8, splitk_for(M, K));
       g.args.out_f32 = dc;
-      g.args.splits = splitk_for(M, K);
       if (g.args.splits > 1) {
         SS_CUDA(cudaMalloc(&dp, sizeof(float) * size_t(g.args.splits) * M * N));
         g.args.partial = dp;

@@ -160,22 +160,35 @@ def nearest_neighbour(train_p: np.ndarray, train_y: np.ndarray, query: np.ndarra
 
 
 class Surrogate:
-    """The trained network plus its empirical error model."""
+    """The trained network plus its empirical error model.  With
+    `standardize`, the network learns each echo point centred and scaled by
+    the training curves' mean and spread at that time, and its outputs are
+    mapped back."""
 
-    def __init__(self, engine: Engine, batch: int = 1024, seed: int = 0):
+    def __init__(self, engine: Engine, batch: int = 1024, seed: int = 0,
+                 standardize: bool = False):
         self.engine = engine
         self.net = Mlp(engine, batch=batch, seed=seed)
+        self.standardize = standardize
+        self.y_mean = np.zeros(POINTS)
+        self.y_scale = np.ones(POINTS)
         self.cal_x: Optional[np.ndarray] = None
         self.cal_p: Optional[np.ndarray] = None
         self.cal_err: Optional[np.ndarray] = None
 
     def fit(self, p: np.ndarray, y: np.ndarray, steps: int, lr_start: float = 2e-3,
             lr_end: float = 1e-5, seed: int = 0) -> np.ndarray:
-        self.net.set_data(features(p), np.asarray(y, dtype=np.float32))
+        y = np.asarray(y, dtype=np.float64)
+        if self.standardize:
+            self.y_mean = y.mean(axis=0)
+            self.y_scale = np.maximum(y.std(axis=0), 1e-6)
+        t = (y - self.y_mean) / self.y_scale
+        self.net.set_data(features(p), t.astype(np.float32))
         return self.net.train(steps, lr_start, lr_end, seed)
 
     def raw(self, p: np.ndarray) -> np.ndarray:
-        return self.net.forward(features(p)).astype(np.float64)
+        out = self.net.forward(features(p)).astype(np.float64)
+        return out * self.y_scale + self.y_mean
 
     def calibrate(self, p: np.ndarray, y: np.ndarray) -> np.ndarray:
         err = np.abs(self.raw(p) - y).max(axis=1)
@@ -214,37 +227,110 @@ class Surrogate:
         return out, use, est
 
 
-def run(args) -> dict:
-    """Generate, train, calibrate and evaluate; returns the report.  Each size
-    gets its own number of points (larger L costs more per curve), split
-    80 / 10 / 10 into training, calibration and test points."""
-    eng = Engine(0)
-    sizes = tuple(args.sizes)
-    counts = list(args.points) if args.points else [args.train + args.cal + args.test] * len(sizes)
-    if len(counts) != len(sizes):
-        raise SystemExit("--points needs one count per size")
-    ranges = {"tau": (args.tau_min, args.tau_max)}
-    rep: dict = {"realizations": args.realizations, "sizes": list(sizes), "points": counts,
-                 "steps": args.steps, "tau_range": list(ranges["tau"])}
-    parts = {"train": [], "cal": [], "test": []}
-    gen = {}
+def split_counts(counts, test_points: int, cal_frac: float = 0.1):
+    """(train, cal, test) points per size: `test_points` held-out points in
+    all, shared in proportion to each size's points (10 % each when 0), and
+    `cal_frac` of every size for calibration."""
+    counts = [int(c) for c in counts]
+    total = sum(counts)
+    if test_points <= 0:
+        test = [int(0.1 * c) for c in counts]
+    else:
+        if test_points >= total:
+            raise SystemExit("--test-points must be below the total number of points")
+        test = [int(round(test_points * c / total)) for c in counts]
+        test[int(np.argmax(counts))] += test_points - sum(test)
+    cal = [int(cal_frac * c) for c in counts]
+    train = [c - a - b for c, a, b in zip(counts, cal, test)]
+    if min(train) <= 0:
+        raise SystemExit("no training points left for a size")
+    return train, cal, test
+
+
+def _max_err(pred: np.ndarray, y: np.ndarray) -> np.ndarray:
+    return np.abs(pred - y).max(axis=1)
+
+
+def _error_summary(pred: np.ndarray, y: np.ndarray) -> dict:
+    err = _max_err(pred, y)
+    return {"rms": float(np.sqrt(((pred - y) ** 2).mean())),
+            "max_err_median": float(np.median(err)),
+            "max_err_p90": float(np.quantile(err, 0.9)),
+            "max_err_max": float(err.max())}
+
+
+def generate(eng: Engine, sizes, counts, realizations: int, seed: int, ranges) -> dict:
+    """Points and exact curves per size (all mixed precision, no routing)."""
+    data, gen = {}, {}
     for k, (L, n) in enumerate(zip(sizes, counts)):
-        p = sample(n, args.seed + 7919 * k, sizes=(L,), ranges=ranges)
+        p = sample(n, seed + 7919 * k, sizes=(L,), ranges=ranges)
         t0 = time.perf_counter()
-        y = exact(eng, p, args.realizations, mixed_order_limit=-1)
+        y = exact(eng, p, realizations, mixed_order_limit=-1)
         dt = time.perf_counter() - t0
-        gen[int(L)] = {"points": n, "seconds": dt, "curves_per_s": n * args.realizations / dt}
-        a, b = int(0.8 * n), int(0.9 * n)
+        gen[int(L)] = {"points": n, "seconds": dt, "curves_per_s": n * realizations / dt}
+        data[int(L)] = (p, y)
+    return {"data": data, "generation": gen}
+
+
+def save_data(path: str, data: dict, realizations: int) -> None:
+    arrays = {"realizations": np.asarray(realizations)}
+    for L, (p, y) in data.items():
+        arrays[f"p{L}"] = p
+        arrays[f"y{L}"] = y.astype(np.float32)
+    np.savez_compressed(path, **arrays)
+
+
+def load_data(path: str):
+    z = np.load(path)
+    data = {}
+    for key in z.files:
+        if key.startswith("p"):
+            L = int(key[1:])
+            data[L] = (z[key], z[f"y{L}"].astype(np.float64))
+    return data, int(z["realizations"])
+
+
+def run(args) -> dict:
+    """Generate (or load), train, calibrate and evaluate; returns the report.
+    Each size gets its own number of points (larger L costs more per curve);
+    the held-out test set is `--test-points` points across the sizes, judged
+    by the exact engine's curves."""
+    eng = Engine(0)
+    ranges = {"tau": (args.tau_min, args.tau_max)}
+    if args.load_data:
+        data, realizations = load_data(args.load_data)
+        sizes = tuple(sorted(data))
+        counts = [len(data[L][0]) for L in sizes]
+        gen = None
+    else:
+        sizes = tuple(args.sizes)
+        counts = list(args.points) if args.points else [args.train + args.cal + args.test] * len(sizes)
+        if len(counts) != len(sizes):
+            raise SystemExit("--points needs one count per size")
+        realizations = args.realizations
+        g = generate(eng, sizes, counts, realizations, args.seed, ranges)
+        data, gen = g["data"], g["generation"]
+        if args.save_data:
+            save_data(args.save_data, data, realizations)
+    ntr, ncal, nte = split_counts(counts, args.test_points)
+    rep: dict = {"realizations": realizations, "sizes": list(sizes), "points": counts,
+                 "train_points": ntr, "cal_points": ncal, "test_points": nte,
+                 "steps": args.steps, "standardize": bool(args.standardize),
+                 "tau_range": list(ranges["tau"])}
+    if gen is not None:
+        rep["generation"] = gen
+    parts = {"train": [], "cal": [], "test": []}
+    for L, a, b in zip(sizes, ntr, ncal):
+        p, y = data[int(L)]
         parts["train"].append((p[:a], y[:a]))
-        parts["cal"].append((p[a:b], y[a:b]))
-        parts["test"].append((p[b:], y[b:]))
-    rep["generation"] = gen
+        parts["cal"].append((p[a:a + b], y[a:a + b]))
+        parts["test"].append((p[a + b:], y[a + b:]))
     cat = {k: (np.concatenate([q for q, _ in v]), np.concatenate([z for _, z in v]))
            for k, v in parts.items()}
     ptr, ytr = cat["train"]
     pcal, ycal = cat["cal"]
     pte, yte = cat["test"]
-    sur = Surrogate(eng, batch=args.batch, seed=args.seed)
+    sur = Surrogate(eng, batch=args.batch, seed=args.seed, standardize=args.standardize)
     t0 = time.perf_counter()
     losses = sur.fit(ptr, ytr, args.steps, args.lr, args.lr_end, seed=args.seed)
     rep["training"] = {"points": int(len(ptr)), "seconds": time.perf_counter() - t0,
@@ -259,27 +345,32 @@ def run(args) -> dict:
     per = {}
     for L in sizes:
         m = pte["nspins"] == L
-        err = np.abs(pred[m] - yte[m]).max(axis=1)
-        nn_err = np.abs(nn[m] - yte[m]).max(axis=1)
         per[int(L)] = {"test_points": int(m.sum()),
-                       "surrogate_rms": float(np.sqrt(((pred[m] - yte[m]) ** 2).mean())),
-                       "surrogate_max_err_median": float(np.median(err)),
-                       "surrogate_max_err_max": float(err.max()),
-                       "nearest_neighbour_rms": float(np.sqrt(((nn[m] - yte[m]) ** 2).mean())),
-                       "nearest_neighbour_max_err_median": float(np.median(nn_err))}
+                       "surrogate": _error_summary(pred[m], yte[m]),
+                       "nearest_neighbour": _error_summary(nn[m], yte[m])}
     rep["test"] = per
-    # The exact engine's own cost on the test points (same realisations).
+    rep["test_all"] = {"test_points": int(len(pte)),
+                       "surrogate": _error_summary(pred, yte),
+                       "nearest_neighbour": _error_summary(nn, yte)}
+    # The exact engine's own cost on a sample of the test points (the same
+    # realisations), for the speed comparison.
+    rng = np.random.default_rng(args.seed)
+    timing = np.sort(rng.choice(len(pte), min(len(pte), args.exact_timing_points),
+                                replace=False))
     t0 = time.perf_counter()
-    exact(eng, pte, args.realizations, mixed_order_limit=-1)
+    again = exact(eng, pte[timing], realizations, mixed_order_limit=-1)
     ex_s = time.perf_counter() - t0
-    rep["exact_points_per_s"] = len(pte) / ex_s
-    rep["surrogate_speedup"] = (len(pte) / inf_s) / (len(pte) / ex_s)
-    err = np.abs(pred - yte).max(axis=1)
+    rep["exact_points_per_s"] = len(timing) / ex_s
+    rep["exact_timing_points"] = int(len(timing))
+    rep["exact_rerun_max_diff"] = float(np.abs(again - yte[timing]).max())
+    rep["surrogate_speedup"] = (len(pte) / inf_s) / rep["exact_points_per_s"]
+    err = _max_err(pred, yte)
     est = sur.estimate_error(pte)
     for tol in (1e-3, 1e-2, 3e-2, 1e-1):
         use = est <= tol
         rep[f"hybrid_tol_{tol:g}"] = {"answered_by_network": float(use.mean()),
-                                      "violations": int(((err > tol) & use).sum())}
+                                      "violations": int(((err > tol) & use).sum()),
+                                      "within_tol_at_all": float((err <= tol).mean())}
     sur.net._destroy()
     eng.close()
     return rep
@@ -301,6 +392,15 @@ def main(argv=None) -> None:
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--lr-end", type=float, default=1e-5)
     ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--test-points", type=int, default=0,
+                    help="held-out points across all sizes (default: 10 %% of each size)")
+    ap.add_argument("--exact-timing-points", type=int, default=256,
+                    help="test points the exact engine is re-timed on")
+    ap.add_argument("--standardize", action="store_true",
+                    help="train on curves centred and scaled per echo point")
+    ap.add_argument("--save-data", type=str, default="", help="write the generated curves (.npz)")
+    ap.add_argument("--load-data", type=str, default="",
+                    help="train on curves written by --save-data instead of generating")
     ap.add_argument("--out", type=str, default="")
     args = ap.parse_args(argv)
     rep = run(args)

@@ -63,3 +63,26 @@ def test_vectorised_nearest_matches_brute_force():
     # fewer reference rows than k: every row, padded with the last index
     small = sg._nearest(ref[:3], q[:7], 5)
     assert small.shape == (7, 5) and set(np.unique(small)) <= {0, 1, 2}
+
+
+def test_split_counts_hold_out_the_requested_points():
+    tr, cal, te = sg.split_counts([32768, 8192, 1536], 4096)
+    assert sum(te) == 4096
+    assert cal == [3276, 819, 153]
+    assert [a + b + c for a, b, c in zip(tr, cal, te)] == [32768, 8192, 1536]
+    # in proportion to each size's points
+    assert te[0] > te[1] > te[2] > 0
+    tr, cal, te = sg.split_counts([1000, 500], 0)
+    assert te == [100, 50] and cal == [100, 50] and tr == [800, 400]
+
+
+def test_saved_curves_load_back(tmp_path):
+    data = {10: (sg.sample(5, 1, sizes=(10,)), np.linspace(0, 1, 5 * sg.POINTS).reshape(5, -1)),
+            12: (sg.sample(3, 2, sizes=(12,)), np.ones((3, sg.POINTS)))}
+    path = tmp_path / "curves.npz"
+    sg.save_data(str(path), data, 64)
+    got, realizations = sg.load_data(str(path))
+    assert realizations == 64 and sorted(got) == [10, 12]
+    for L in (10, 12):
+        assert np.array_equal(got[L][0], data[L][0])
+        assert np.allclose(got[L][1], data[L][1], atol=1e-7)
