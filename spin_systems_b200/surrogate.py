@@ -33,13 +33,14 @@ from __future__ import annotations
 import argparse
 import json
 import math
+import sys
 import time
 from pathlib import Path
 from typing import Callable, Optional
 
 import numpy as np
 
-from . import Batch, Engine, Mlp, abi
+from . import Batch, ConvergenceError, Engine, Mlp, abi
 from .abi import AXES3, Evolve, Measure, Pulse, Repeat, RunSpec
 
 SEED = 20240726
@@ -77,29 +78,35 @@ def features(p: np.ndarray) -> np.ndarray:
     return x
 
 
-def program(sequence: int, points: int = POINTS):
+def program(sequence: int, points: int = POINTS, substeps: int = 1):
+    """The pulse program; every free evolution is split into `substeps`
+    equal propagation steps (the same evolution: a realisation with a very
+    close pair needs shorter steps for the Chebyshev series to converge)."""
+    def free(fraction):
+        return Evolve(fraction / substeps, steps=substeps, tau_from_draw=True)
     if sequence == 0:
-        body = [Evolve(1.0, tau_from_draw=True), Pulse(math.pi, AXES3["y"]),
-                Evolve(1.0, tau_from_draw=True), Measure()]
+        body = [free(1.0), Pulse(math.pi, AXES3["y"]), free(1.0), Measure()]
         return [Pulse(0.5 * math.pi, AXES3["x"]), Repeat(points, body)]
     body = []
     for a in "XYXYYXYX":
-        body += [Evolve(0.5, tau_from_draw=True), Pulse(math.pi, AXES3[a.lower()]),
-                 Evolve(0.5, tau_from_draw=True), Measure()]
+        body += [free(0.5), Pulse(math.pi, AXES3[a.lower()]), free(0.5), Measure()]
     return [Pulse(0.5 * math.pi, AXES3["x"]), Repeat(points // 8, body)]
 
 
 def sweep_spec(sequence: int, nspins: int, rows, realizations: int,
-               mixed_order_limit: int = 0) -> RunSpec:
-    return RunSpec(nspins=nspins, steps=program(sequence), observables=["corr:x", "norm"],
-                   realizations=realizations, seed=SEED, reference_axis="x",
-                   sweep=rows, mixed_order_limit=mixed_order_limit)
+               mixed_order_limit: int = 0, substeps: int = 1) -> RunSpec:
+    return RunSpec(nspins=nspins, steps=program(sequence, substeps=substeps),
+                   observables=["corr:x", "norm"], realizations=realizations, seed=SEED,
+                   reference_axis="x", sweep=rows, mixed_order_limit=mixed_order_limit)
 
 
 def exact(engine: Engine, p: np.ndarray, realizations: int, precision: int = abi.MIXED,
           max_batch: int = 32768, mixed_order_limit: int = 0) -> np.ndarray:
     """The exact propagator's disorder-averaged echo [n][128] for each point,
-    run as batched sweeps (one batch per sequence and L, chunked)."""
+    run as batched sweeps (one batch per sequence and L, chunked).  A chunk
+    whose strongest realisation's series does not converge within the order
+    limit at one step per free evolution is set up again with 2, 4, ... 64
+    steps per evolution."""
     out = np.zeros((len(p), POINTS))
     per_batch = max(1, max_batch // realizations)
     for seq in np.unique(p["sequence"]):
@@ -109,9 +116,18 @@ def exact(engine: Engine, p: np.ndarray, realizations: int, precision: int = abi
                 sel = idx[at:at + per_batch]
                 rows = [(float(q["density"]) ** 1.5, float(q["sigma"]), float(q["tau"]),
                          1.0 + float(q["angle_error"])) for q in p[sel]]
-                spec = sweep_spec(int(seq), int(L), rows, realizations, mixed_order_limit)
-                cfg = spec.config()
-                b = Batch(engine, cfg, 0, len(sel) * realizations, precision)
+                substeps = 1
+                while True:
+                    spec = sweep_spec(int(seq), int(L), rows, realizations, mixed_order_limit,
+                                      substeps)
+                    cfg = spec.config()
+                    try:
+                        b = Batch(engine, cfg, 0, len(sel) * realizations, precision)
+                        break
+                    except ConvergenceError:
+                        if substeps >= 64:
+                            raise
+                        substeps *= 2
                 _, r = b.run()
                 b._destroy()
                 echo = r[:, :, 0] / (r[:, :, 3] ** 2)
@@ -259,8 +275,10 @@ def _error_summary(pred: np.ndarray, y: np.ndarray) -> dict:
             "max_err_max": float(err.max())}
 
 
-def generate(eng: Engine, sizes, counts, realizations: int, seed: int, ranges) -> dict:
-    """Points and exact curves per size (all mixed precision, no routing)."""
+def generate(eng: Engine, sizes, counts, realizations: int, seed: int, ranges,
+             save: str = "") -> dict:
+    """Points and exact curves per size (all mixed precision, no routing);
+    with `save`, the curves so far are written after every size."""
     data, gen = {}, {}
     for k, (L, n) in enumerate(zip(sizes, counts)):
         p = sample(n, seed + 7919 * k, sizes=(L,), ranges=ranges)
@@ -269,6 +287,10 @@ def generate(eng: Engine, sizes, counts, realizations: int, seed: int, ranges) -
         dt = time.perf_counter() - t0
         gen[int(L)] = {"points": n, "seconds": dt, "curves_per_s": n * realizations / dt}
         data[int(L)] = (p, y)
+        print(f"L = {L}: {n} points x {realizations} realisations in {dt:.0f} s",
+              file=sys.stderr, flush=True)
+        if save:
+            save_data(save, data, realizations)
     return {"data": data, "generation": gen}
 
 
@@ -308,10 +330,8 @@ def run(args) -> dict:
         if len(counts) != len(sizes):
             raise SystemExit("--points needs one count per size")
         realizations = args.realizations
-        g = generate(eng, sizes, counts, realizations, args.seed, ranges)
+        g = generate(eng, sizes, counts, realizations, args.seed, ranges, args.save_data)
         data, gen = g["data"], g["generation"]
-        if args.save_data:
-            save_data(args.save_data, data, realizations)
     ntr, ncal, nte = split_counts(counts, args.test_points)
     rep: dict = {"realizations": realizations, "sizes": list(sizes), "points": counts,
                  "train_points": ntr, "cal_points": ncal, "test_points": nte,

@@ -86,3 +86,23 @@ def test_saved_curves_load_back(tmp_path):
     for L in (10, 12):
         assert np.array_equal(got[L][0], data[L][0])
         assert np.allclose(got[L][1], data[L][1], atol=1e-7)
+
+
+def test_split_programs_keep_the_evolution_and_the_measurements():
+    from spin_systems_b200.abi import Evolve, Repeat
+
+    for seq in (0, 1):
+        one, four = sg.program(seq), sg.program(seq, substeps=4)
+
+        def evolves(prog):
+            out = []
+            for st in prog:
+                if isinstance(st, Repeat):
+                    out += [(e.tau, e.steps) for e in st.body if isinstance(e, Evolve)]
+            return out
+        a, b = evolves(one), evolves(four)
+        assert len(a) == len(b)
+        for (t1, n1), (t4, n4) in zip(a, b):
+            assert n1 == 1 and n4 == 4 and abs(t1 - t4 * n4) < 1e-15
+        spec = sg.sweep_spec(seq, 10, [(1.0, 0.5, 0.3, 1.0)], 4, substeps=4)
+        assert spec.measurement_count() == sg.POINTS
