@@ -135,17 +135,19 @@ def _subgroup_main(rank, world, port, data, total, out):
                             world_size=world, timeout=timedelta(seconds=60))
     try:
         sub = dist.new_group([1, 2])
-        if rank == 0:
-            return
-        d = np.load(data)
-        times, rows = d["times"], d["rows"]
-        res = run_sharded(lambda first, count: (times, rows[first:first + count]), total,
-                          group=sub)
-        if rank == 1:
-            t, acc = res
-            np.savez(out, times=t, mean=acc.mean, count=acc.count)
-        else:
-            assert res is None
+        if rank != 0:
+            d = np.load(data)
+            times, rows = d["times"], d["rows"]
+            res = run_sharded(lambda first, count: (times, rows[first:first + count]), total,
+                              group=sub)
+            if rank == 1:
+                t, acc = res
+                np.savez(out, times=t, mean=acc.mean, count=acc.count)
+            else:
+                assert res is None
+        # Rank 0 hosts the rendezvous store that the subgroup still uses:
+        # it leaves only after the other two are done.
+        dist.barrier()
     finally:
         dist.destroy_process_group()
 
