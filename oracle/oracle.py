@@ -388,7 +388,50 @@ def dense_pauli(L: int, spin: int, axis: str) -> np.ndarray:
     return out
 
 
+def _pauli_string(L: int, ops) -> tuple:
+    """Row index and value of each column k of a product of single-spin
+    Paulis on distinct spins, ops = [(spin, axis), ...]: the product maps
+    basis state k to one basis state with a phase, so it is a column
+    permutation with a factor (the same matrix as the kron product of
+    dense_pauli, without forming it)."""
+    k = np.arange(1 << L)
+    row = k.copy()
+    val = np.ones(1 << L, dtype=complex)
+    for spin, axis in ops:
+        b = (k >> spin) & 1
+        m = _PAULI[axis]
+        nb = b ^ 1 if axis in "xy" else b
+        val = val * m[nb, b]
+        if axis in "xy":
+            row = row ^ (1 << spin)
+    return row, val
+
+
 def dense_hamiltonian(L: int, fields, pairs, J) -> np.ndarray:
+    """The dense matrix of Hamiltonian.cpp:95-127's H: sum of h_a / 2 sigma_a
+    per spin and J_a / 4 sigma_a sigma_a per pair, assembled term by term as
+    phased permutations (tests.test_oracle_pins checks it against the kron
+    construction)."""
+    H = np.zeros((1 << L, 1 << L), dtype=complex)
+    cols = np.arange(1 << L)
+    f = np.asarray(fields).reshape(L, 3)
+    for s in range(L):
+        for a, ax in enumerate("xyz"):
+            if f[s, a] != 0.0:
+                row, val = _pauli_string(L, [(s, ax)])
+                H[row, cols] += 0.5 * f[s, a] * val
+    pr = np.asarray(pairs).reshape(-1, 2)
+    jj = np.asarray(J).reshape(-1, 3)
+    for (lo, hi), j in zip(pr, jj):
+        for a, ax in enumerate("xyz"):
+            if j[a] != 0.0:
+                row, val = _pauli_string(L, [(int(lo), ax), (int(hi), ax)])
+                H[row, cols] += 0.25 * j[a] * val
+    return H
+
+
+def dense_hamiltonian_kron(L: int, fields, pairs, J) -> np.ndarray:
+    """dense_hamiltonian by explicit kron products (small L only)."""
     H = np.zeros((1 << L, 1 << L), dtype=complex)
     f = np.asarray(fields).reshape(L, 3)
     for s in range(L):

@@ -286,6 +286,7 @@ def plain(args) -> dict:
               ("mixed", abi.MIXED, "gather", abi.KERNEL_GATHER, 0)]
     combos += [("fp64", abi.FP64, "tiled", abi.KERNEL_TILED, r) for r in args.fp64_bits]
     combos += [("mixed", abi.MIXED, "tiled", abi.KERNEL_TILED, r) for r in args.mixed_bits]
+    default_fp64 = f"tiled_r{args.fp64_bits[0]}" if args.fp64_bits else "tiled_r3"
     for L in args.sizes:
         spec = workloads.long_propagation(nspins=L, steps=1, every=1, epsilon=1e-7)
         cfg = spec.config()
@@ -323,7 +324,7 @@ def plain(args) -> dict:
             final[(pname, kname)] = psi.download()
             out[f"{pname}_{kname}"] = r
             del psi
-        ref = final.get(("fp64", "gather"), final.get(("fp64", "tiled_r3")))
+        ref = final.get(("fp64", "gather"), final.get(("fp64", default_fp64)))
         for key, v in final.items():
             if ref is not None and key != ("fp64", "gather"):
                 out[f"{key[0]}_{key[1]}"]["max_dev_vs_fp64"] = float(np.abs(v - ref).max())
@@ -425,7 +426,8 @@ def main(argv=None) -> None:
     pl.add_argument("--steps", type=int, default=2)
     pl.add_argument("--skip", nargs="*", default=[], help="kernel families to leave out")
     pl.add_argument("--fp64-bits", type=int, nargs="+", default=[3, 4],
-                    help="register bits of the FP64 tiled schedules to time")
+                    help="register bits of the FP64 tiled schedules to time (the first is "
+                         "the reference for the deviations when the gather kernel is skipped)")
     pl.add_argument("--mixed-bits", type=int, nargs="+", default=[4, 5],
                     help="register bits of the mixed tiled schedules to time")
     pl.add_argument("--gather-max", type=int, default=30,

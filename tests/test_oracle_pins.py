@@ -16,7 +16,8 @@ import math
 import numpy as np
 import pytest
 
-from oracle.oracle import (dense_exp_apply, dense_hamiltonian, dense_pauli, random_state,
+from oracle.oracle import (dense_exp_apply, dense_hamiltonian, dense_hamiltonian_kron,
+                           dense_pauli, random_state,
                            sample_hamiltonian, to_complex, to_interleaved)
 from spin_systems_b200 import abi, workloads
 
@@ -110,6 +111,14 @@ def test_imaginary_time_matches_dense_exponential(port):
     for tau in (0.05, 0.4):
         psi, _ = port.evolve(L, f, p, J, psi0, 1, tau, 1, eps=1e-12)
         assert np.abs(to_complex(psi) - to_complex(dense_exp_apply(H, tau, psi0))).max() < 1e-10
+
+
+def test_dense_hamiltonian_matches_the_kron_products():
+    # The permutation assembly against explicit kron products of the
+    # single-spin matrices, every axis on fields and pairs.
+    for L in range(1, 7):
+        f, p, J = sample_hamiltonian(L)
+        assert np.array_equal(dense_hamiltonian(L, f, p, J), dense_hamiltonian_kron(L, f, p, J))
 
 
 def test_dense_pauli_algebra():

@@ -43,21 +43,23 @@ def test_tiled_fp64_matches_the_reference_propagator(engine, port, kernel, sizes
         assert np.abs(got - gather).max() < 1e-12, (L, np.abs(got - gather).max())
 
 
-@pytest.mark.parametrize("precision,bits", [(abi.FP64, 4), (abi.MIXED, 5)])
+@pytest.mark.parametrize("precision,bits", [(abi.FP64, 3), (abi.FP64, 4), (abi.MIXED, 4),
+                                           (abi.MIXED, 5)])
 def test_every_tiled_schedule_matches(engine, port, precision, bits):
-    # The non-default schedules (register bits per thread) against the
-    # reference propagator (FP64) or the FP64 gather kernel (mixed).
-    L = 14
-    f, p, J = sample_hamiltonian(L)
-    psi0 = random_state(L, 0x5C4E)
+    # Every schedule (register bits per thread) against the reference
+    # propagator, on a Hamiltonian with transverse fields and flip-both
+    # terms, at sizes of one to eight tiles.
+    tol = 1e-10 if precision == abi.FP64 else 1e-6
     ss.tiled_select(precision, bits)
     try:
-        got, _ = propagate(engine, L, f, p, J, psi0, TILED, precision)
+        for L in (13, 15):
+            f, p, J = sample_hamiltonian(L)
+            psi0 = random_state(L, 0x5C4E + L)
+            got, _ = propagate(engine, L, f, p, J, psi0, TILED, precision)
+            want, _ = port.evolve(L, f, p, J, psi0, abi.REAL, 0.1, 2, eps=1e-12)
+            assert np.abs(got - want).max() < tol, (L, np.abs(got - want).max())
     finally:
         ss.tiled_select(precision, 0)
-    want, _ = port.evolve(L, f, p, J, psi0, abi.REAL, 0.1, 2, eps=1e-12)
-    tol = 1e-10 if precision == abi.FP64 else 1e-6
-    assert np.abs(got - want).max() < tol
     with pytest.raises(ss.InvalidArgumentError):
         ss.tiled_select(abi.FP64, 5)
 
