@@ -1780,6 +1780,7 @@ extern "C" {
 int ss_batch_create(ss_engine* engine, const ss_run_config* config, uint64_t first, int64_t count,
                     int precision, ss_batch** out) {
   return guarded([&] {
+    TraceRange trace("ss_batch_create");
     require(engine != nullptr && config != nullptr && out != nullptr, SS_ERR_INVALID_ARGUMENT,
             "null argument");
     require(count >= 1, SS_ERR_INVALID_ARGUMENT, "an ensemble needs at least one realisation");
@@ -1848,6 +1849,7 @@ int ss_batch_upload(ss_batch* b) {
 
 int ss_batch_execute(ss_batch* b) {
   return guarded([&] {
+    TraceRange trace("ss_batch_execute");
     require(b != nullptr, SS_ERR_INVALID_ARGUMENT, "null batch");
     execute(b);
   });
@@ -1862,6 +1864,7 @@ int ss_batch_download(ss_batch* b, double* rows, double* times) {
 
 int ss_batch_run(ss_batch* b, double* rows, double* times) {
   return guarded([&] {
+    TraceRange trace("ss_batch_run");
     require(b != nullptr, SS_ERR_INVALID_ARGUMENT, "null batch");
     upload(b);
     execute(b);
@@ -2033,6 +2036,7 @@ extern "C" {
 int ss_batch_tune(ss_engine* e, const ss_run_config* config, uint64_t first, int64_t sample,
                   int precision, const char* cache_path) {
   return guarded([&] {
+    TraceRange trace("ss_batch_tune");
     require(e != nullptr && config != nullptr, SS_ERR_INVALID_ARGUMENT, "null argument");
     require(sample >= 1, SS_ERR_INVALID_ARGUMENT, "the tuning sample needs a realisation");
     require(precision == SS_PRECISION_FP64 || precision == SS_PRECISION_MIXED,

@@ -7,9 +7,23 @@
 #include <stdexcept>
 #include <string>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/spinsim_b200.h"
 
 namespace ss {
+
+// A named NVTX range over one host call of the C ABI (batch execution, a
+// propagation, a training run): a marker on a profiler's timeline and a
+// filter for `ncu --nvtx --nvtx-include`.  NVTX is header-only and the push
+// and pop cost a pointer check unless a tool is attached.
+class TraceRange {
+ public:
+  explicit TraceRange(const char* name) { nvtxRangePushA(name); }
+  ~TraceRange() { nvtxRangePop(); }
+  TraceRange(const TraceRange&) = delete;
+  TraceRange& operator=(const TraceRange&) = delete;
+};
 
 struct Error : std::runtime_error {
   int code;

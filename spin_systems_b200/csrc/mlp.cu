@@ -1156,6 +1156,7 @@ int ss_mlp_set_data(ss_mlp* n, const float* x, const float* y, int64_t rows) {
 int ss_mlp_train(ss_mlp* n, int64_t steps, float lr_start, float lr_end, uint64_t seed,
                  double* losses) {
   return guarded([&] {
+    TraceRange trace("ss_mlp_train");
     check_mlp(n);
     require(n->data_n >= n->batch, SS_ERR_INVALID_ARGUMENT, "no training set (ss_mlp_set_data)");
     require(steps >= 0, SS_ERR_INVALID_ARGUMENT, "negative step count");

@@ -291,6 +291,7 @@ int ss_evolve_ex(const ss_ham* hc, ss_state* psi, const double* coeffs, int64_t 
                  double bound, int mode, int64_t nsteps, int autonormalize, int precision,
                  int kernel) {
   return guarded([&] {
+    TraceRange trace("ss_evolve");
     auto* h = const_cast<ss_ham*>(hc);
     check_ham(h);
     check_state(psi);
@@ -316,6 +317,7 @@ int ss_propagate_ex(const ss_ham* hc, ss_state* psi, int mode, double tau, int64
                     int autonormalize, double epsilon, int precision, int kernel,
                     int64_t* order_used) {
   return guarded([&] {
+    TraceRange trace("ss_propagate");
     auto* h = const_cast<ss_ham*>(hc);
     check_ham(h);
     check_state(psi);

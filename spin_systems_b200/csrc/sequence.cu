@@ -215,6 +215,7 @@ using namespace ss;
 extern "C" int ss_run_realization(ss_engine* engine, const ss_run_config* config, uint64_t index,
                                   double* times, double* values) {
   return guarded([&] {
+    TraceRange trace("ss_run_realization");
     require(engine != nullptr && config != nullptr && times != nullptr && values != nullptr,
             SS_ERR_INVALID_ARGUMENT, "null argument");
     run_realization_plain(engine, *config, index, times, values, SS_PRECISION_FP64,
@@ -226,6 +227,7 @@ extern "C" int ss_run_realization_ex(ss_engine* engine, const ss_run_config* con
                                      uint64_t index, int precision, int kernel, double* times,
                                      double* values) {
   return guarded([&] {
+    TraceRange trace("ss_run_realization");
     require(engine != nullptr && config != nullptr && times != nullptr && values != nullptr,
             SS_ERR_INVALID_ARGUMENT, "null argument");
     run_realization_plain(engine, *config, index, times, values, precision, kernel);

@@ -48,6 +48,34 @@ def corr0(cfg, idx, lmax):
     return np.array(out)
 
 
+def plain_time_model(raw: dict, amps: dict) -> dict:
+    """The plain path's time for every realisation of each size from a timed
+    sample: least squares seconds = fixed + rate x amplitude-orders over the
+    size's sample (both clamped at zero), summed over the size's
+    realisations.  A per-realisation fixed cost (host set-up, graph capture
+    of each new expansion) makes seconds per amplitude-order fall with the
+    work, so scaling the sample's mean rate by the size's amplitude-orders
+    would overstate the heavy realisations that carry most of them."""
+    per, total = {}, 0.0
+    for L, r in raw.items():
+        x = np.asarray(r["amplitude_orders"], dtype=np.float64)
+        y = np.asarray(r["seconds"], dtype=np.float64)
+        if len(x) >= 2 and np.ptp(x) > 0:
+            rate, fixed = np.polyfit(x, y, 1)
+        else:
+            rate, fixed = float(y.mean() / x.mean()), 0.0
+        if fixed < 0.0:
+            fixed, rate = 0.0, float((x * y).sum() / (x * x).sum())
+        if rate < 0.0:
+            fixed, rate = float(y.mean()), 0.0
+        a = np.asarray(amps[L], dtype=np.float64)
+        sec = float(len(a) * fixed + rate * a.sum())
+        per[int(L)] = {"fixed_seconds": float(fixed), "ns_per_amp_order": float(rate * 1e9),
+                       "seconds": sec, "realizations": int(len(a))}
+        total += sec
+    return {"seconds": total, "per_size": per}
+
+
 def uneven(args) -> dict:
     eng = Engine(0)
     spec = workloads.cpmg_uneven(realizations=args.realizations)
@@ -73,29 +101,28 @@ def uneven(args) -> dict:
     e1.record(stream)
     e1.synchronize()
     dev_s = e0.elapsed_time(e1) / 1e3 / args.steps
-    t0 = time.perf_counter()
-    _, mixed = b.run()
-    e2e_s = time.perf_counter() - t0
+    if args.e2e:
+        t0 = time.perf_counter()
+        _, mixed = b.run()
+        e2e_s = time.perf_counter() - t0
+    else:
+        _, mixed = b.download()
+        e2e_s = float("nan")
     rep = {"workload": "uneven CPMG-32, L in {8,10,12,14,16}, sigma, tau ~ U[0.1,1]",
            "realizations": n, "per_size": {int(L): int((sizes == L).sum()) for L in np.unique(sizes)},
            "batched_mixed": {"seconds_per_batch": dev_s, "curves_per_s": n / dev_s,
-                             "e2e_curves_per_s": n / e2e_s,
+                             "e2e_curves_per_s": n / e2e_s if args.e2e else None,
                              "amplitude_orders": stats["amplitude_orders"],
                              "fp64_routed": int((prec == abi.FP64).sum()),
                              "create_seconds": create_s},
            "schedule": [{k: r[k] for k in ("L", "precision", "variant", "ns")} for r in table],
            "tuning_seconds": tune_s}
     # The FP64 reference: the plain path on a sample of each size, which also
-    # gives the echo error of those curves.
-    # The sample of each size is spread over its work distribution: the
-    # size's realisations sorted by amplitude-orders, one taken at evenly
-    # spaced ranks (lightest to heaviest).
-    errs = {}
-    plain = {}
-    samples = {}
-    spread = {}
-    per_size_rate = {}  # seconds per amplitude-order of each sampled curve
-    per_size_time = {}  # the size's realisations times the sample's mean seconds
+    # gives the echo error of those curves.  The sample of each size is
+    # spread over its work distribution: the size's realisations sorted by
+    # amplitude-orders, one taken at evenly spaced ranks (lightest to
+    # heaviest).
+    errs, samples, raw = {}, {}, {}
     for L in np.unique(sizes):
         members = np.flatnonzero(sizes == L)
         order = members[np.argsort(amp[members], kind="stable")]
@@ -112,36 +139,31 @@ def uneven(args) -> dict:
             _, ref = run_realization(eng, cfg, int(i), b.points, b.width)
             ts.append(time.perf_counter() - t0)
             es.append(float(np.abs(mixed[i, :, 0] - ref[:, 0]).max() / scale[j]))
-        rate = np.array(ts) / amp[idx]
-        per_size_rate[int(L)] = (members, rate)
-        per_size_time[int(L)] = len(members) * float(np.mean(ts))
-        plain[int(L)] = float(rate.mean() * amp[members].mean())
+        raw[int(L)] = {"index": [int(i) for i in idx], "amplitude_orders": amp[idx].tolist(),
+                       "seconds": ts}
         samples[int(L)] = int(len(idx))
-        spread[int(L)] = {"ns_per_amp_order_min": float(rate.min() * 1e9),
-                          "ns_per_amp_order_max": float(rate.max() * 1e9),
-                          "ns_per_amp_order_cv": float(rate.std() / rate.mean())}
         errs[int(L)] = {"max": max(es), "mean": float(np.mean(es))}
-    # The batch's plain time: each size's amplitude-orders times its sampled
-    # mean seconds per amplitude-order; a bootstrap over the samples gives the
-    # spread of the ratio.
-    def plain_total_for(pick):
-        return sum(float(amp[m].sum()) * float(r[pick(r)].mean()) for m, r in per_size_rate.values())
-    plain_total = plain_total_for(lambda r: np.arange(len(r)))
+    amps = {int(L): amp[sizes == L] for L in np.unique(sizes)}
+    model = plain_time_model(raw, amps)
+    plain_total = model["seconds"]
     rng = np.random.default_rng(20240726)
-    boots = [plain_total_for(lambda r: rng.integers(0, len(r), len(r))) for _ in range(2000)]
-    ratio = (n / dev_s) / (n / plain_total)
-    lo, hi = np.percentile([(n / dev_s) / (n / t) for t in boots], [2.5, 97.5])
-    rep["plain_fp64"] = {"seconds_per_realization": plain, "sampled": samples,
-                         "spread": spread, "curves_per_s": n / plain_total,
+    boots = []
+    for _ in range(2000):
+        pick = {}
+        for L, r in raw.items():
+            j = rng.integers(0, len(r["seconds"]), len(r["seconds"]))
+            pick[L] = {"amplitude_orders": np.asarray(r["amplitude_orders"])[j],
+                       "seconds": np.asarray(r["seconds"])[j]}
+        boots.append(plain_time_model(pick, amps)["seconds"])
+    lo, hi = np.percentile([t / dev_s for t in boots], [2.5, 97.5])
+    rep["plain_fp64"] = {"curves_per_s": n / plain_total, "seconds_per_batch": plain_total,
+                         "per_size": model["per_size"], "sampled": samples, "samples": raw,
                          "note": "one realisation at a time through ss_run_realization on a "
-                                 "sample of each size spread over its amplitude-orders; the "
-                                 "size's time is its amplitude-orders times the sample's mean "
-                                 "seconds per amplitude-order"}
-    rep["speedup_batched_mixed_over_plain_fp64"] = ratio
-    # Cross-check without the per-amplitude-order model: each size's count
-    # times its sample's mean seconds per realisation (the sample is spread
-    # evenly over the size's ranks by work).
-    rep["speedup_from_mean_seconds"] = (n / dev_s) / (n / sum(per_size_time.values()))
+                                 "sample of each size spread over its amplitude-orders; each "
+                                 "size's time from a least-squares fit of seconds = fixed + "
+                                 "rate x amplitude-orders over its sample, applied to every "
+                                 "realisation of the size"}
+    rep["speedup_batched_mixed_over_plain_fp64"] = plain_total / dev_s
     rep["speedup_95pct_bootstrap"] = [float(lo), float(hi)]
     rep["echo_error_vs_plain_fp64"] = errs
     b._destroy()
@@ -413,7 +435,9 @@ def main(argv=None) -> None:
     u.add_argument("--warmup", type=int, default=0,
                    help="untimed runs first (the graph is instantiated at creation)")
     u.add_argument("--tune-sample", type=int, default=64)
-    u.add_argument("--plain-sample", type=int, default=8)
+    u.add_argument("--plain-sample", type=int, default=16)
+    u.add_argument("--no-e2e", dest="e2e", action="store_false", default=True,
+                   help="skip the end-to-end run through ss_batch_run")
     u.add_argument("--out", default="")
     lo = sub.add_parser("long")
     lo.add_argument("--nspins", type=int, default=16)
