@@ -625,6 +625,12 @@ def main():
         run_reference_arm(args)
     else:
         run_ours(args)
+    # Under torchrun every rank leaves the process group it joined (no CUDA
+    # graph holds a collective, so nothing is left in flight).
+    if "torch.distributed" in sys.modules:
+        import torch.distributed as dist
+        if dist.is_available() and dist.is_initialized():
+            dist.destroy_process_group()
 
 
 if __name__ == "__main__":
