@@ -5,19 +5,29 @@
 // Chebyshev expansions over a range of sizes and arguments.
 //
 //   host_check [--expect-errors] config.toml ...
+//   host_check --csv rows.txt
 //
 // Every file must load and validate, or with --expect-errors every file must
 // be rejected with a ConfigError (malformed input).  Prints one summary line
 // and exits 0; a sanitizer finding aborts the process with its own report.
+//
+// With --csv the checker instead folds measurement rows through the C++ API's
+// Accumulator in index order and prints writeCsv's output.  rows.txt holds
+// "points columns realisations", the column names, the times, then one line
+// of points x columns values per realisation (decimal, round-tripping every
+// double).
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <exception>
+#include <fstream>
+#include <iostream>
 #include <string>
 #include <vector>
 
 #include "../host_numerics.hpp"
 #include "spinsim/io/Config.hpp"
+#include "spinsim/io/Experiment.hpp"
 
 namespace {
 
@@ -108,9 +118,37 @@ int checkNumerics() {
   return failures;
 }
 
+// Rows -> Accumulator (index order) -> writeCsv on standard output.
+int foldRows(const char* path) {
+  std::ifstream in(path);
+  std::size_t points = 0, ncols = 0, count = 0;
+  if (!(in >> points >> ncols >> count) || points == 0 || ncols == 0 || count == 0) {
+    std::fprintf(stderr, "%s: bad header\n", path);
+    return 1;
+  }
+  spinsim::EnsembleResult result;
+  result.columns.resize(ncols);
+  for (std::string& c : result.columns) in >> c;
+  result.times.resize(points);
+  for (double& t : result.times) in >> t;
+  result.statistics = spinsim::Accumulator(points * ncols);
+  std::vector<double> row(points * ncols);
+  for (std::size_t r = 0; r < count; ++r) {
+    for (double& v : row) in >> v;
+    if (!in) {
+      std::fprintf(stderr, "%s: short row %zu\n", path, r);
+      return 1;
+    }
+    result.statistics.add(row);
+  }
+  spinsim::writeCsv(result, std::cout);
+  return 0;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
+  if (argc == 3 && std::strcmp(argv[1], "--csv") == 0) return foldRows(argv[2]);
   bool expectErrors = false;
   std::vector<std::string> paths;
   for (int i = 1; i < argc; ++i) {

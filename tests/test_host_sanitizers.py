@@ -53,3 +53,31 @@ def test_host_layer_under_sanitizers(tmp_path):
     r = _run(["--expect-errors", *bad])
     assert r.returncode == 0, r.stdout + r.stderr
     assert f"{len(bad)} config(s) rejected as expected" in r.stdout
+
+
+def test_statistics_and_csv_are_the_references_bytes(tmp_path):
+    # The C++ API's Accumulator and writeCsv (under the sanitizers), fed the
+    # L = 10 CPMG rows of the C restatement, which are bit-identical to the
+    # reference's curves, print the reference's own runExperiment + writeCsv
+    # output byte for byte (tests/golden/reference_csv.json; Welford in index
+    # order, {:.10g} times, {:.12g} statistics; io/Experiment.cpp:74-110).
+    import json
+
+    from oracle.oracle import Port
+    from spin_systems_b200 import workloads
+
+    subprocess.run(["make", "-s", "-C", str(CSRC), "host-check"], check=True, timeout=900)
+    want = json.loads((ROOT / "tests" / "golden" / "reference_csv.json").read_text())["cpmg_l10"]
+    spec = workloads.cpmg_ideal()
+    times, rows, _ = Port().run_range(spec.config(), 0, spec.realizations, 4)
+    header = want.splitlines()[0].split(",")[1:]
+    columns = [h[: -len("_mean")] for h in header[0::3]]
+    n, points, width = rows.shape
+    assert width == len(columns) and points == len(times)
+    lines = [f"{points} {width} {n}", " ".join(columns), " ".join(repr(float(t)) for t in times)]
+    lines += [" ".join(repr(float(v)) for v in r.ravel()) for r in rows]
+    src = tmp_path / "rows.txt"
+    src.write_text("\n".join(lines) + "\n")
+    r = _run(["--csv", src])
+    assert r.returncode == 0, r.stderr
+    assert r.stdout == want
